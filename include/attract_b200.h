@@ -1,0 +1,195 @@
+/*
+ * attract_b200 -- C ABI of the B200 (sm_100a) ATTRACT scoring + rigid-body
+ * minimisation path.
+ *
+ * Every pointer named *_dev is a caller-owned device buffer; the library does
+ * not allocate device memory.  Every call is asynchronous on the given CUDA
+ * stream and returns an int status: ATT_OK (0) or an ATT_E_* code, with a
+ * message in att_last_error_string() (thread-local).  Nothing aborts or traps.
+ *
+ * Reference interface each entry point replaces (paths within
+ * sjdv1982/attract-jax):
+ *   att_energrad         main()/main0() + value_and_grad,  test5.py:404-429
+ *                        (and the 4x4-matrix form of test1.py:361-366,409-412)
+ *   att_minimise         the batch/epoch optimiser loop, test5.py:436-467
+ *                        (optax.adam form of test4.py:440-455)
+ *   att_energrad_backward  reverse mode of test5.py:429, extended to the grid
+ *                        values (no counterpart: JAX never differentiates the grid)
+ *   att_grid_repack      the dense grid arrays of read_grid2.py:92-155
+ *                        -> the brick layout the kernels read
+ *   att_build_potential_grid  calc_grid(), test-calc-grid-energy.py:154-196
+ *   att_nbgrid_count / att_nbgrid_fill  the neighbour lists of
+ *                        test-calc-grid-energy.py:90-103 (KD-tree query)
+ */
+#ifndef ATTRACT_B200_H
+#define ATTRACT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ATT_OK 0
+#define ATT_E_INVALID 1     /* bad argument (shape, range, alignment, NULL) */
+#define ATT_E_CUDA 2        /* a CUDA runtime call failed */
+#define ATT_E_UNSUPPORTED 3 /* configuration not built into this library */
+
+#define ATT_MAX_GRIDS 8
+#define ATT_NB_EMPTY 65535u /* empty neighbour-list slot (read_grid2.py:118) */
+
+/* grad_mode */
+#define ATT_GRAD_REFERENCE 0 /* grid gradient = -interpolated stored force (test5.py:310),
+                                nb gradient with the plateau correction (test5.py:220-229) */
+#define ATT_GRAD_ANALYTIC 1  /* exact derivative of the computed energy */
+
+/* flags */
+#define ATT_FLAG_TRILINEAR_QUIRK 1 /* reference floor/ceil weights: a bead with an exactly
+                                      integer voxel coordinate reads 0 (test5.py:256-259) */
+
+/* per-pose status bits written by att_minimise / att_energrad */
+#define ATT_STATUS_NONFINITE_GRAD 1   /* a step saw a non-finite gradient and was skipped */
+#define ATT_STATUS_NONFINITE_ENERGY 2 /* the returned energy is not finite */
+
+/* Geometry of one receptor grid: the scalar fields of read_grid2.py's Grid. */
+typedef struct AttGridGeom {
+  float origin[3];  /* position of inner grid point (0,0,0) */
+  float spacing;    /* gridspacing (inner); the outer grid has 2*spacing */
+  int dim[3];       /* inner grid points per axis */
+  int dim2[3];      /* outer grid points per axis */
+  int extension;    /* gridextension: outer point j sits at origin + (2j - extension)*spacing */
+  float plateau;    /* plateaudis: pair terms apply for d < plateau */
+  int n_types;      /* potential slots (ligand grid types) */
+  int pad_;
+} AttGridGeom;
+
+/* One receptor, resident on the device (all pointers *_dev). */
+typedef struct AttGrid {
+  AttGridGeom geom;
+  const void* bricks;          /* float4 [n_types][n_inner_bricks + n_outer_bricks][8]; 128-B aligned;
+                                  NULL = no potential grid (neighbour grid only) */
+  long long n_inner_bricks;    /* (dim[0]-1)(dim[1]-1)(dim[2]-1) */
+  long long n_outer_bricks;    /* (dim2[0]-1)(dim2[1]-1)(dim2[2]-1), 0 = no outer grid */
+  const uint32_t* nb_hdr;      /* [dim0*dim1*dim2][2] = {start, count} per inner grid point; NULL = none */
+  const uint16_t* nb_list;     /* receptor bead index per entry (ATT_NB_EMPTY skipped) */
+  long long n_nb_entries;
+  const float* rec;            /* [n_rec][4] x, y, z, receptor type (as an int32 bit pattern) */
+  int n_rec;
+  int n_rtypes;                /* receptor types in the pair table */
+  int n_ltypes;                /* ligand types in the pair table */
+  int pad_;
+  const float* pair;           /* [n_ltypes][n_rtypes][8]: rc, ac, emin, rmin2, ivor, eplat, gplat, rcap2 */
+} AttGrid;
+
+/* Ligands: all beads of all ligands concatenated. */
+typedef struct AttLigands {
+  const float* beads;   /* [n_beads][4] x, y, z, type word = gtype | (ltype << 16) (int32 bits) */
+  const int* offset;    /* [n_lig + 1] first bead of each ligand */
+  int n_lig;
+  int max_beads;        /* max over ligands of offset[l+1]-offset[l] */
+} AttLigands;
+
+/* A run of consecutive poses scored against one grid with one ligand. */
+typedef struct AttSegment {
+  int grid;     /* index into the grids array */
+  int lig;      /* ligand index (base index when pose_lig is given) */
+  int pose0;    /* first pose of the run */
+  int n_poses;
+} AttSegment;
+
+typedef struct AttEvalCfg {
+  int grad_mode;    /* ATT_GRAD_* */
+  int flags;        /* ATT_FLAG_* */
+  float gravity;    /* adds gravity*|t|^2 (test5.py:419 uses 0.1) */
+  int pose_format;  /* 0: [B][6] phi,psi,theta,tx,ty,tz ; 1: [B][16] row-vector 4x4 (test5.py:413-415) */
+} AttEvalCfg;
+
+typedef struct AttAdamCfg {
+  AttEvalCfg eval;
+  float lr_rot;     /* rad */
+  float lr_trans;   /* Angstrom */
+  float beta1, beta2, eps;
+  int step0;        /* steps already taken by the given adam_state (bias correction) */
+} AttAdamCfg;
+
+/* Launch shape; zeros pick the defaults / autotuned values. */
+typedef struct AttLaunchCfg {
+  int lanes_per_pose;   /* 8, 16 or 32 (poses per warp = 32 / lanes_per_pose) */
+  int block_threads;    /* multiple of 32, <= 1024 */
+  int blocks;           /* persistent CTAs (att_minimise), 0 = fill the GPU */
+  int pad_;
+} AttLaunchCfg;
+
+const char* att_last_error_string(void);
+const char* att_version(void);
+
+/* Bytes of float4 bricks needed for a grid: n_types*(n_inner+n_outer)*128. */
+long long att_grid_brick_bytes(const AttGridGeom* geom, int with_outer);
+
+/* Dense reference grids -> bricks.  inner_dev: float [n_types][dim0][dim1][dim2][4],
+   outer_dev: [n_types][dim2_0][dim2_1][dim2_2][4] or NULL.  (read_grid2.py:92-155) */
+int att_grid_repack(const AttGridGeom* geom, const float* inner_dev, const float* outer_dev,
+                    void* bricks_dev, void* stream);
+
+/* One energy (+gradient) evaluation of every pose of every segment.
+   pose_dev [B][6] (or [B][16]); pose_lig_dev [B] optional per-pose ligand offset (conformers);
+   energy_dev [B]; grad_dev [B][6] (Euler) or [B][16] dE/dmat (pose_format 1), may be NULL;
+   status_dev [B] optional.  test5.py:404-429. */
+int att_energrad(const AttGrid* grids, int n_grids, const AttLigands* ligs,
+                 const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
+                 const float* pose_dev, const int* pose_lig_dev, const AttEvalCfg* cfg,
+                 float* energy_dev, float* grad_dev, int* status_dev,
+                 const AttLaunchCfg* launch, void* stream);
+
+/* Fused rigid-body ADAM minimisation: `steps` evaluate+update iterations, then a
+   final evaluation whose energy is returned.  pose_in_dev/pose_out_dev [B][6] (may
+   alias); adam_state_dev [B][12] (m[6], v[6]) in/out or NULL (start from zero);
+   work_counter_dev: one int of scratch, zeroed by this call; stats_dev: optional
+   [3] u64 counters (bead evaluations, neighbour lookups, list entries visited).
+   seg_tile_dev [n_segs+1]: first work tile of each segment (a tile is
+   32/lanes_per_pose consecutive poses of one segment).  test5.py:436-467. */
+int att_minimise(const AttGrid* grids, int n_grids, const AttLigands* ligs,
+                 const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
+                 const float* pose_in_dev, float* pose_out_dev, const int* pose_lig_dev,
+                 float* adam_state_dev, const AttAdamCfg* cfg, int steps,
+                 float* energy_dev, int* status_dev, int* work_counter_dev,
+                 unsigned long long* stats_dev, const AttLaunchCfg* launch, void* stream);
+
+/* Adjoint of att_energrad for L = sum_b dL_dE[b] * E[b]: dL/dpose [B][6] and the
+   scatter-add of dL/d(grid energy values) into dgrid_inner_dev / dgrid_outer_dev,
+   float [n_types][dim..][4] (channel 0 receives the gradient; the caller zeroes
+   the buffers).  Recomputes the forward instead of storing per-bead weights. */
+int att_energrad_backward(const AttGrid* grids, int n_grids, const AttLigands* ligs,
+                          const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
+                          const float* pose_dev, const int* pose_lig_dev, const AttEvalCfg* cfg,
+                          const float* dL_dE_dev, float* dL_dpose_dev,
+                          float* dgrid_inner_dev, float* dgrid_outer_dev,
+                          const AttLaunchCfg* launch, void* stream);
+
+/* Potential grid of energies and forces for ligand types 0..n_ltypes-1 at the inner
+   (outer=0) or outer (outer=1) grid points: per receptor bead within `cutoff`,
+   the pair energy and force beyond the plateau, the plateau energy and the plateau
+   force along d inside it.  pair_dev as in AttGrid.pair but carrying the plateau
+   values of this geometry.  out_dev float [n_ltypes][dim..][4].
+   test-calc-grid-energy.py:154-196. */
+int att_build_potential_grid(const AttGridGeom* geom, const float* rec_dev, int n_rec,
+                             const float* pair_dev, int n_rtypes, int n_ltypes, float cutoff,
+                             int outer, float* out_dev, void* stream);
+
+/* Neighbour lists of receptor beads within `radius` of every inner grid point,
+   ascending bead index.  att_nbgrid_count writes hdr_dev [V][2] = {start, count}
+   and the entry total (one u64 on the device); it needs
+   att_nbgrid_workspace_bytes(V) bytes of scratch.  att_nbgrid_fill then writes
+   the entries.  test-calc-grid-energy.py:90-103. */
+long long att_nbgrid_workspace_bytes(long long n_voxels);
+int att_nbgrid_count(const AttGridGeom* geom, const float* rec_dev, int n_rec, float radius,
+                     uint32_t* hdr_dev, unsigned long long* total_dev, void* workspace_dev,
+                     long long workspace_bytes, void* stream);
+int att_nbgrid_fill(const AttGridGeom* geom, const float* rec_dev, int n_rec, float radius,
+                    const uint32_t* hdr_dev, uint16_t* list_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ATTRACT_B200_H */

@@ -1,0 +1,83 @@
+"""Seeded small cases shared by the GPU parity tests: grids, ligands and poses
+that exercise the inner grid, the outer grid, the space outside both, the
+neighbour lists and the pair-table branches."""
+from __future__ import annotations
+
+import numpy as np
+
+import attract_oracle as O
+
+
+def small_case(seed=0, n_types=4, n_rtypes=3, n_rec=60, n_lig_beads=9, n_poses=64, cap=True, ivor_mix=False,
+               plateau=3.5, spacing=1.0, with_outer=True, with_grid=True, with_nb=True):
+    rng = np.random.default_rng(seed)
+    dim = np.array([14, 13, 12])
+    ext = 4
+    dim2 = np.array([11, 10, 10])
+    origin = np.array([-6.5, -6.0, -5.5])
+    geom = dict(origin=origin, spacing=spacing, dim=dim, dim2=dim2, extension=ext, plateau=plateau)
+    sigma = rng.uniform(2.0, 3.0, (n_rtypes, n_types))
+    eps = rng.uniform(0.1, 2.0, (n_rtypes, n_types))
+    rc, ac = eps * sigma ** 8, eps * sigma ** 6
+    ivor = np.ones_like(rc)
+    if ivor_mix:
+        ivor = np.where(rng.random(rc.shape) < 0.5, -1.0, 1.0)
+    rcap2 = (0.6 * sigma) ** 2 if cap else np.zeros_like(sigma)
+    box_lo = origin + 1.0
+    box_hi = origin + (dim - 2) * spacing
+    rec = rng.uniform(box_lo, box_hi, (n_rec, 3))
+    rtype = rng.integers(0, n_rtypes, n_rec)
+    pair = O.pair_table(rc, ac, ivor, plateau, shift_plateau=with_grid, rcap2=rcap2)
+    G = dict(geom=geom, rec=rec, rtype=rtype, pair=pair)
+    if with_grid:
+        G["inner"] = rng.normal(size=(n_types, *dim, 4))
+        if with_outer:
+            G["outer"] = rng.normal(size=(n_types, *dim2, 4))
+    if with_nb:
+        G["nb_hdr"], G["nb_list"] = O.build_nbgrid(rec, geom, plateau + spacing * np.sqrt(3) / 2 + 0.05)
+    lig = O.transform(np.zeros(6), rng.normal(size=(n_lig_beads, 3)) * 1.6)
+    lig -= lig.mean(0)
+    gt = rng.integers(0, n_types, n_lig_beads)
+    lt = rng.integers(0, n_types, n_lig_beads)
+    ang = rng.uniform(-np.pi, np.pi, (n_poses, 3))
+    centre = origin + (dim - 1) * spacing / 2
+    # most poses inside the inner grid, some straddling into the outer grid or beyond
+    r = np.where(rng.random(n_poses) < 0.75, rng.uniform(0, 4.0, n_poses), rng.uniform(5.0, 14.0, n_poses))
+    d = rng.normal(size=(n_poses, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    t = centre + d * r[:, None]
+    poses = np.concatenate([ang, t], 1)
+    f32 = lambda a: np.asarray(a, np.float32).astype(np.float64)
+    G["rec"] = f32(G["rec"])
+    for k in ("inner", "outer"):
+        if k in G:
+            G[k] = f32(G[k])
+    lig, poses = f32(lig), f32(poses)
+    return dict(G=G, lig=lig, gt=gt, lt=lt, poses=poses, rc=rc, ac=ac, ivor=ivor, rcap2=rcap2,
+                n_types=n_types, n_rtypes=n_rtypes, with_grid=with_grid)
+
+
+def to_device_grid(case, device="cuda"):
+    """The case's grid as an attract_b200 Grid (same arrays as the oracle sees)."""
+    from attract_b200 import ForceField, Grid, GridGeom
+
+    G = case["G"]
+    g = G["geom"]
+    geom = GridGeom(tuple(g["origin"]), g["spacing"], tuple(g["dim"]), tuple(g["dim2"]), g["extension"],
+                    g["plateau"], case["n_types"])
+    ff = ForceField(case["rc"], case["ac"], case["ivor"], case["rcap2"])
+    return Grid.from_dense(geom, G["rec"], G["rtype"], ff, inner=G.get("inner"), outer=G.get("outer"),
+                           nb_hdr=G.get("nb_hdr"), nb_list=G.get("nb_list"), shift_plateau=case["with_grid"],
+                           keep_dense=True, device=device)
+
+
+def oracle_scales(case, poses, mode="reference", quirk=True):
+    """Per-pose magnitude scales for float32 tolerances: sum over beads of |E_b|
+    and of |dE/dx_b| * (1 + |r_b|)."""
+    G = case["G"]
+    X = O.transform(poses, case["lig"])
+    Eb, gb = O.bead_energrad(X, case["gt"], case["lt"], G, mode, quirk)
+    r = X - poses[:, None, 3:6]
+    es = np.abs(Eb).sum(1)
+    gs = (np.linalg.norm(gb, axis=2) * (1 + np.linalg.norm(r, axis=2))).sum(1)
+    return es, gs

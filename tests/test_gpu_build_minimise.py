@@ -1,0 +1,183 @@
+"""GPU builders (K3/K4/K5), the fused minimiser and batching against the oracle."""
+import numpy as np
+import pytest
+import torch
+
+import attract_oracle as O
+from gpu_cases import small_case, to_device_grid
+
+pytestmark = pytest.mark.gpu
+
+
+def _A():
+    import attract_b200 as A
+
+    A.load_library()
+    return A
+
+
+def _small_receptor(seed=0, n=40, n_types=4):
+    A = _A()
+    rng = np.random.default_rng(seed)
+    ff = A.ForceField.synthetic(n_types, seed)
+    geom = A.GridGeom((-8.0, -7.5, -7.0), 1.0, (17, 16, 15), (12, 12, 11), 4, 3.0, n_types)
+    xyz = rng.uniform(-5, 5, (n, 3)).astype(np.float32).astype(np.float64)
+    t = rng.integers(0, n_types, n)
+    return A, ff, geom, xyz, t
+
+
+def test_potential_grid_builder_vs_oracle():
+    A, ff, geom, xyz, t = _small_receptor()
+    g = A.Grid.build(xyz, t, ff, geom, cutoff=6.0, keep_dense=True)
+    inner, outer, _, _ = g.dense_host()
+    pair = O.pair_table(ff.rc, ff.ac, ff.ivor, geom.plateau, True, ff.rcap2)
+    gd = geom.as_dict()
+    ref_in = O.build_potential_grid(xyz, t, pair, gd, geom.n_types, 6.0, outer=False)
+    ref_out = O.build_potential_grid(xyz, t, pair, gd, geom.n_types, 6.0, outer=True)
+    for got, ref in ((inner, ref_in), (outer, ref_out)):
+        scale = np.abs(ref).max(axis=(1, 2, 3), keepdims=True)
+        # grid points exactly at the cutoff radius are the only float32/float64 disagreements
+        bad = np.abs(got - ref) > 1e-6 * scale + 1e-6
+        assert bad.mean() < 1e-4, bad.mean()
+
+
+def test_nbgrid_builder_vs_oracle():
+    A, ff, geom, xyz, t = _small_receptor(seed=1)
+    radius = 3.0 + np.sqrt(3) / 2 + 0.01
+    g = A.Grid.build(xyz, t, ff, geom, list_radius=radius, potentials=False)
+    _, _, hdr, lst = g.dense_host()
+    ref_hdr, ref_lst = O.build_nbgrid(xyz, geom.as_dict(), radius)
+    assert np.array_equal(hdr[:, 0], np.cumsum(hdr[:, 1]) - hdr[:, 1])  # CSR starts
+    if not (np.array_equal(hdr, ref_hdr) and np.array_equal(lst[: len(ref_lst)], ref_lst)):
+        # only pairs within float32 rounding of the radius may differ
+        pts = O.grid_points(geom.as_dict()).reshape(-1, 3)
+        d = np.linalg.norm(pts[:, None, :] - xyz[None], axis=2)
+        got = np.zeros_like(d, dtype=bool)
+        for v in range(len(hdr)):
+            s, n = hdr[v]
+            got[v, lst[s:s + n]] = True
+        mismatch = got != (d <= radius)
+        assert np.all(np.abs(d[mismatch] - radius) < 1e-4)
+
+
+def test_repack_bricks_exact():
+    A = _A()
+    c = small_case(seed=11, n_poses=4)
+    grid = to_device_grid(c)
+    ref = O.repack_bricks(c["G"]["inner"].astype(np.float32), c["G"]["outer"].astype(np.float32))
+    got = grid.bricks.cpu().numpy()
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref)
+
+
+def _minimise_case(seed=12, n_poses=64, lanes=8):
+    A = _A()
+    c = small_case(seed=seed, n_poses=n_poses)
+    grid = to_device_grid(c)
+    ligs = A.LigandSet([(c["lig"], c["gt"], c["lt"])])
+    wl = A.Workload([grid], ligs, [A.Segment(0, 0, n_poses)], lanes_per_pose=lanes)
+    return A, c, wl
+
+
+def test_minimise_one_step_matches_oracle():
+    A, c, wl = _minimise_case()
+    P = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+    out, E, S, _ = A.minimise(wl, P, 1)
+    xo, Eo, fo = O.minimise(c["poses"], c["lig"], c["gt"], c["lt"], c["G"], 1)
+    d = np.abs(out.cpu().numpy() - xo)
+    # one ADAM step moves each DOF by ~lr*sign(g): a sign decided by float32
+    # noise (|g| tiny) may flip; everything else agrees to float32 precision
+    assert np.mean(d < 1e-4) > 0.97, np.mean(d < 1e-4)
+
+
+def test_minimise_many_steps_ranking():
+    A, c, wl = _minimise_case(seed=13, n_poses=128)
+    P = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+    out, E, S, _ = A.minimise(wl, P, 40)
+    xo, Eo, fo = O.minimise(c["poses"], c["lig"], c["gt"], c["lt"], c["G"], 40)
+    E = E.cpu().numpy()
+    assert np.all(np.isfinite(E))
+    from scipy.stats import spearmanr
+
+    assert spearmanr(E, Eo).correlation > 0.98
+    close = np.abs(E - Eo) <= 1e-3 * np.maximum(np.abs(Eo), 1.0)
+    assert close.mean() > 0.8, close.mean()
+    # the energy reported is the energy of the pose returned
+    Ef, _, _ = A.energrad(wl, out.contiguous())
+    assert np.allclose(Ef.cpu().numpy(), E, rtol=1e-6, atol=1e-5)
+
+
+def test_minimise_lanes_identical():
+    res = []
+    for lanes in (8, 16, 32):
+        A, c, wl = _minimise_case(seed=14, n_poses=50, lanes=lanes)
+        P = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+        out, E, _, _ = A.minimise(wl, P, 10)
+        res.append((out.cpu().numpy(), E.cpu().numpy()))
+    for o, e in res[1:]:
+        assert np.allclose(o, res[0][0], rtol=1e-5, atol=1e-5)
+        assert np.allclose(e, res[0][1], rtol=1e-4, atol=1e-4)
+
+
+def test_minimise_resume_with_adam_state_is_exact():
+    A, c, wl = _minimise_case(seed=15, n_poses=40)
+    P = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+    full, Ef, _, _ = A.minimise(wl, P, 10)
+    st = torch.zeros((40, 12), dtype=torch.float32, device="cuda")
+    half, _, _, _ = A.minimise(wl, P, 5, adam_state=st)
+    rest, Er, _, _ = A.minimise(wl, half.clone(), 5, A.AdamOptions(step0=5), adam_state=st)
+    assert torch.equal(full, rest)
+    assert torch.equal(Ef, Er)
+
+
+def test_batched_uneven_equals_alone():
+    """Many ligands of uneven sizes in one launch give bit-identical results to
+    each ligand minimised alone."""
+    A = _A()
+    base = small_case(seed=16, n_poses=8)
+    grid = to_device_grid(base)
+    rng = np.random.default_rng(3)
+    ligs, segs, poses = [], [], []
+    for i, n in enumerate((3, 9, 17, 30)):
+        lig = rng.normal(size=(n, 3)) * 1.5
+        lig -= lig.mean(0)
+        ligs.append((lig, rng.integers(0, 4, n), rng.integers(0, 4, n)))
+        k = 5 + 7 * i
+        segs.append(A.Segment(0, i, k))
+        poses.append(small_case(seed=20 + i, n_poses=k)["poses"])
+    L = A.LigandSet(ligs)
+    wl = A.Workload([grid], L, segs)
+    P = torch.tensor(np.concatenate(poses), dtype=torch.float32, device="cuda")
+    out, E, _, _ = A.minimise(wl, P, 12)
+    out, E = out.cpu().numpy(), E.cpu().numpy().copy()
+    off = 0
+    for i, s in enumerate(segs):
+        wl1 = A.Workload([grid], A.LigandSet([ligs[i]]), [A.Segment(0, 0, s.n_poses)])
+        o1, E1, _, _ = A.minimise(wl1, P[off:off + s.n_poses].contiguous(), 12)
+        assert np.array_equal(o1.cpu().numpy(), out[off:off + s.n_poses])
+        assert np.array_equal(E1.cpu().numpy(), E[off:off + s.n_poses])
+        off += s.n_poses
+
+
+def test_graph_capture_replay_matches_direct():
+    A, c, wl = _minimise_case(seed=17, n_poses=64)
+    plan = A.MinimisePlan(wl, 8)
+    plan.pose_in.copy_(torch.tensor(c["poses"], dtype=torch.float32))
+    out1, E1, _, _ = plan.run()
+    o1, e1 = out1.clone(), E1.clone()
+    plan.capture()
+    for _ in range(2):
+        out2, E2, _ = plan.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(o1, out2) and torch.equal(e1, E2)
+
+
+def test_minimise_stats_counts():
+    A, c, wl = _minimise_case(seed=18, n_poses=32)
+    P = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+    _, _, _, st = A.minimise(wl, P, 3, stats=True)
+    st = st.cpu().numpy()
+    n_lig = len(c["lig"])
+    assert 0 < st[0] <= 4 * 32 * n_lig
+    assert 0 < st[1] <= 4 * 32 * n_lig
+    assert st[2] >= 0

@@ -1,0 +1,224 @@
+"""CUDA path (through the C ABI) against the oracle on identical inputs.
+
+Tolerances (float32 kernels vs the float64 oracle):
+* energy per pose: |dE| <= 1e-5 * S_E + 1e-4 kcal/mol, S_E = sum over beads of
+  |E_bead| (float32 summation error is bounded relative to the sum of
+  magnitudes, not to a cancelling total);
+* gradient per pose and component: |dg| <= 1e-4 * S_g + 1e-3, S_g = sum over
+  beads of |dE/dx_b| (1 + |r_b|) (torques carry the lever arm r_b).
+"""
+import numpy as np
+import pytest
+import torch
+
+import attract_oracle as O
+from conftest import dat_poses, mono_leu_setup
+from gpu_cases import oracle_scales, small_case, to_device_grid
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine():
+    import attract_b200 as A
+
+    A.load_library()
+    return A
+
+
+def _wl(A, grid, lig, gt, lt, n, lanes=8):
+    ligs = A.LigandSet([(lig, gt, lt)])
+    return A.Workload([grid], ligs, [A.Segment(0, 0, n)], lanes_per_pose=lanes)
+
+
+def _check(E, G, Eo, Go, es, gs):
+    dE = np.abs(E - Eo)
+    assert np.all(dE <= 1e-5 * es + 1e-4), (dE.max(), np.argmax(dE - 1e-5 * es))
+    if G is not None:
+        dG = np.abs(G - Go)
+        tol = 1e-4 * gs[:, None] + 1e-3
+        assert np.all(dG <= tol), (dG.max(), np.unravel_index(np.argmax(dG - tol), dG.shape))
+
+
+@pytest.mark.parametrize("mode", ["reference", "analytic"])
+@pytest.mark.parametrize("lanes", [8, 16, 32])
+def test_energrad_small_grid(mode, lanes):
+    A = _engine()
+    c = small_case(seed=1, n_poses=96)
+    grid = to_device_grid(c)
+    wl = _wl(A, grid, c["lig"], c["gt"], c["lt"], len(c["poses"]), lanes)
+    poses = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+    E, G, S = A.energrad(wl, poses, A.EvalOptions(grad_mode=mode))
+    torch.cuda.synchronize()
+    Eo, Go = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], c["G"], mode=mode)
+    es, gs = oracle_scales(c, c["poses"], mode)
+    _check(E.cpu().numpy(), G.cpu().numpy(), Eo, Go, es, gs)
+    assert np.all(S.cpu().numpy() == 0)
+
+
+def test_energrad_branches_ivor_nocap_gravity():
+    A = _engine()
+    c = small_case(seed=2, n_poses=64, cap=False, ivor_mix=True)
+    grid = to_device_grid(c)
+    wl = _wl(A, grid, c["lig"], c["gt"], c["lt"], len(c["poses"]))
+    poses = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+    E, G, _ = A.energrad(wl, poses, A.EvalOptions(gravity=0.1))
+    Eo, Go = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], c["G"], gravity=0.1)
+    es, gs = oracle_scales(c, c["poses"])
+    t = c["poses"][:, 3:]
+    es = es + 0.1 * (t * t).sum(1)
+    gs = gs + 0.2 * np.abs(t).max(1)
+    _check(E.cpu().numpy(), G.cpu().numpy(), Eo, Go, es, gs)
+
+
+@pytest.mark.parametrize("what", ["grid_only", "nb_only", "inner_only"])
+def test_energrad_partial_grids(what):
+    A = _engine()
+    kw = dict(grid_only=dict(with_nb=False), nb_only=dict(with_grid=False), inner_only=dict(with_outer=False))[what]
+    c = small_case(seed=3, n_poses=64, **kw)
+    grid = to_device_grid(c)
+    wl = _wl(A, grid, c["lig"], c["gt"], c["lt"], len(c["poses"]))
+    poses = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+    E, G, _ = A.energrad(wl, poses)
+    Eo, Go = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], c["G"])
+    es, gs = oracle_scales(c, c["poses"])
+    _check(E.cpu().numpy(), G.cpu().numpy(), Eo, Go, es, gs)
+
+
+def test_trilinear_quirk_integer_voxels():
+    """A bead on an exactly integer voxel coordinate reads 0 with the reference
+    weights (test5.py:256-259) and the grid value without them."""
+    A = _engine()
+    c = small_case(seed=4, n_poses=8, with_nb=False)
+    g = c["G"]["geom"]
+    lig = np.zeros((1, 3))
+    poses = np.zeros((8, 6))
+    rng = np.random.default_rng(0)
+    idx = rng.integers(1, 8, (8, 3)).astype(np.float64)
+    idx[4:, 0] += 0.25  # x non-integer, y/z integer: still a quirk zero
+    poses[:, 3:] = g["origin"] + idx * g["spacing"]
+    grid = to_device_grid(c)
+    wl = _wl(A, grid, lig, np.array([1]), np.array([1]), 8)
+    P = torch.tensor(poses, dtype=torch.float32, device="cuda")
+    for quirk in (True, False):
+        E, _, _ = A.energrad(wl, P, A.EvalOptions(quirk=quirk))
+        Eo, _ = O.energrad(poses, lig, np.array([1]), np.array([1]), c["G"], quirk=quirk)
+        assert np.allclose(E.cpu().numpy(), Eo, rtol=1e-5, atol=1e-5)
+        if quirk:
+            assert np.all(Eo == 0.0)
+        else:
+            assert np.all(Eo != 0.0)
+
+
+def test_mat_pose_format_and_consistency():
+    A = _engine()
+    c = small_case(seed=5, n_poses=32)
+    grid = to_device_grid(c)
+    wl = _wl(A, grid, c["lig"], c["gt"], c["lt"], 32)
+    mats = O.pose_to_mat(c["poses"])
+    E, dM, _ = A.energrad(wl, torch.tensor(mats, dtype=torch.float32, device="cuda"))
+    Eo, dMo = O.energrad_mat(mats, c["lig"], c["gt"], c["lt"], c["G"])
+    es, gs = oracle_scales(c, c["poses"])
+    assert np.all(np.abs(E.cpu().numpy() - Eo) <= 1e-5 * es + 1e-4)
+    d = np.abs(dM.cpu().numpy() - dMo).reshape(32, -1)
+    assert np.all(d <= 1e-4 * gs[:, None] + 1e-3)
+
+
+def test_edge_cases_empty_outside_nan():
+    A = _engine()
+    c = small_case(seed=6, n_poses=8)
+    grid = to_device_grid(c)
+    ligs = A.LigandSet([(c["lig"], c["gt"], c["lt"])])
+    # empty segment between two others, a lone pose, poses far outside every grid
+    wl = A.Workload([grid], ligs, [A.Segment(0, 0, 3), A.Segment(0, 0, 0), A.Segment(0, 0, 1)])
+    poses = np.zeros((4, 6))
+    poses[:, 3:] = 1e4
+    poses[3, 0] = np.nan
+    E, G, S = A.energrad(wl, torch.tensor(poses, dtype=torch.float32, device="cuda"))
+    E, G, S = E.cpu().numpy(), G.cpu().numpy(), S.cpu().numpy()
+    assert np.all(E[:3] == 0) and np.all(G[:3] == 0) and np.all(S[:3] == 0)
+    assert S[3] == 0 or np.isfinite(E[3])  # NaN angles place nothing on a grid: no term applies
+    wl0 = A.Workload([grid], ligs, [A.Segment(0, 0, 0)])
+    E0, _, _ = A.energrad(wl0, torch.zeros((0, 6), dtype=torch.float32, device="cuda"))
+    assert E0.numel() == 0
+
+
+def test_host_validation_errors():
+    A = _engine()
+    c = small_case(seed=7, n_poses=4)
+    grid = to_device_grid(c)
+    with pytest.raises(ValueError):
+        A.Workload([grid], A.LigandSet([(c["lig"], c["gt"] + 10, c["lt"])]), [A.Segment(0, 0, 4)])
+    with pytest.raises(ValueError):
+        A.Workload([grid] * 9, A.LigandSet([(c["lig"], c["gt"], c["lt"])]), [A.Segment(0, 0, 4)])
+    wl = _wl(A, grid, c["lig"], c["gt"], c["lt"], 4)
+    with pytest.raises(ValueError):
+        A.energrad(wl, torch.zeros((5, 6), dtype=torch.float32, device="cuda"))
+
+
+# --------------------------------------------------------------------------- golden
+@pytest.fixture(scope="module")
+def mono(golden):
+    A = _engine()
+    out = {}
+    for shift in (False, True):
+        G = mono_leu_setup(golden, shift_plateau=shift)
+        g = G["geom"]
+        rbc, abc, ipon = golden["par15"]
+        ff = A.ForceField([[abc * rbc ** 8]], [[abc * rbc ** 6]], [[ipon]])
+        geom = A.GridGeom(tuple(g["origin"]), g["spacing"], tuple(int(x) for x in g["dim"]),
+                          tuple(int(x) for x in g["dim2"]), 0, g["plateau"], 1)
+        grid = A.Grid.from_dense(geom, G["rec"], G["rtype"], ff, nb_hdr=G["nb_hdr"], nb_list=G["nb_list"],
+                                 shift_plateau=shift)
+        out[shift] = (G, grid)
+    return out
+
+
+def test_golden_nbgrid_score_attract(golden, mono):
+    """ATTRACT's own neighbour-grid scores (minim-sorted-nbgrid.score): energies
+    and -dE/d(euler, t), through the kernel."""
+    A = _engine()
+    G, grid = mono[False]
+    beads = golden["beads"]
+    z = np.zeros(len(beads), int)
+    wl = _wl(A, grid, beads, z, z, 64)
+    poses = dat_poses(golden)
+    E, Gr, _ = A.energrad(wl, torch.tensor(poses, dtype=torch.float32, device="cuda"))
+    E, Gr = E.cpu().numpy().astype(np.float64), Gr.cpu().numpy().astype(np.float64)
+    refE, refG = golden["score_nbgrid_energy"], golden["score_nbgrid_grad"]
+    assert np.all(np.abs(E - refE) <= 2e-4 * np.abs(refE) + 5e-3)
+    err = np.linalg.norm(-Gr - refG, axis=1) / np.linalg.norm(refG, axis=1)
+    assert np.median(err) < 1e-4 and err.max() < 1e-3, (np.median(err), err.max())
+
+
+def test_golden_vs_oracle_fp64(golden, mono):
+    A = _engine()
+    beads = golden["beads"]
+    z = np.zeros(len(beads), int)
+    poses = dat_poses(golden).astype(np.float32).astype(np.float64)
+    for shift in (False, True):
+        G, grid = mono[shift]
+        wl = _wl(A, grid, beads, z, z, 64)
+        E, Gr, _ = A.energrad(wl, torch.tensor(poses, dtype=torch.float32, device="cuda"))
+        Eo, Go = O.energrad(poses, beads.astype(np.float32).astype(np.float64), z, z, G)
+        dE = np.abs(E.cpu().numpy() - Eo)
+        assert np.all(dE <= 1e-5 * np.abs(Eo) + 2e-3), dE.max()
+        gn = np.linalg.norm(Go, axis=1)
+        assert np.all(np.linalg.norm(Gr.cpu().numpy() - Go, axis=1) <= 1e-4 * gn + 1e-2)
+
+
+def test_golden_jax_plateau_out(golden, mono):
+    """test-nb-energrad-plateau.out: test5 semantics through the kernel (4x4 poses)."""
+    A = _engine()
+    _, grid = mono[True]
+    beads = golden["beads"]
+    z = np.zeros(len(beads), int)
+    wl = _wl(A, grid, beads, z, z, 10)
+    E, dM, _ = A.energrad(wl, torch.tensor(golden["mat10"], dtype=torch.float32, device="cuda"))
+    E, dM = E.cpu().numpy(), dM.cpu().numpy()
+    i = [0, 1, 2, 3, 4, 5, 7, 8, 9]
+    refE = golden["jax_nbplat_energy"][i]
+    assert np.all(np.abs(E[i] - refE) <= 2e-5 * np.abs(refE) + 3e-3)
+    refT = golden["jax_nbplat_negdt"][i]
+    assert np.all(np.abs(-dM[i, 3, :3] - refT) <= 1e-4 * np.abs(refT) + 5e-3)
+    refM = golden["jax_nbplat_negdM"][i]
+    assert np.all(np.abs(-dM[i, :3, :3] - refM) <= 2e-5 * np.abs(refM).max((1, 2))[:, None, None])

@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .grid import Grid
+from .grid import Grid, _dev
 from .ligand import LigandSet
 
 
@@ -94,7 +94,7 @@ class Workload:
             raise ValueError(f"1..{_lib.ATT_MAX_GRIDS} grids per launch, got {len(grids)}")
         if lanes_per_pose not in (8, 16, 32):
             raise ValueError("lanes_per_pose must be 8, 16 or 32")
-        self.device = torch.device(device if device is not None else grids[0].device)
+        self.device = _dev(device if device is not None else grids[0].device)
         self.grids = list(grids)
         self.ligands = ligands
         self.segments = [Segment(*s) for s in segments]

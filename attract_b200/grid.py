@@ -79,7 +79,11 @@ class GridGeom:
 
 
 def _dev(device):
-    return torch.device(device if device is not None else "cuda")
+    """A torch.device with its index resolved (``cuda`` -> ``cuda:<current>``)."""
+    d = torch.device(device if device is not None else "cuda")
+    if d.type == "cuda" and d.index is None:
+        d = torch.device("cuda", torch.cuda.current_device())
+    return d
 
 
 def pack_receptor(xyz, rtype, device) -> torch.Tensor:

@@ -12,6 +12,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .grid import _dev
 
 
 class LigandSet:
@@ -19,7 +20,7 @@ class LigandSet:
         """``ligands``: list of ``(xyz [N,3], gtype [N], ltype [N])`` (ltype may be None = gtype)."""
         if len(ligands) == 0:
             raise ValueError("no ligands")
-        self.device = torch.device(device if device is not None else "cuda")
+        self.device = _dev(device)
         rows, offs, self.sizes = [], [0], []
         self.host = []
         for xyz, gt, lt in ligands:

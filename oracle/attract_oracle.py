@@ -280,7 +280,7 @@ def grid_energrad(pos, gtype, geom, inner, outer, quirk=True, mode="reference", 
 # neighbour-grid pair term (test5.py:208-253, 322-349)
 # --------------------------------------------------------------------------
 def nb_energrad(pos, ltype, geom, nb_hdr, nb_list, rec, rtype, pair, mode="reference",
-                dtype=np.float64):
+                dtype=np.float64, absolute=False):
     """Per-bead nbgrid pair energy and dE/dx.
 
     The list is looked up at the nearest inner-grid point ``floor(v+0.5)`` of a
@@ -289,7 +289,8 @@ def nb_energrad(pos, ltype, geom, nb_hdr, nb_list, rec, rtype, pair, mode="refer
     the gradient of the custom JVP, ``2 d (dnonbon - gplat * p/|d|)``
     (test5.py:220-229).  ``mode='analytic'`` drops the plateau correction of
     the gradient (the exact derivative of the energy).  ``nb_hdr`` is
-    ``[n_voxels, 2]`` (start, count) into ``nb_list``.
+    ``[n_voxels, 2]`` (start, count) into ``nb_list``.  ``absolute=True`` sums
+    |term| instead of term (magnitude scales for float32 tolerances).
     """
     dt = np.dtype(dtype)
     pos = np.asarray(pos, dt)
@@ -333,8 +334,11 @@ def nb_energrad(pos, ltype, geom, nb_hdr, nb_list, rec, rtype, pair, mode="refer
         gfac = dt.type(2) * (gmain - gplat * p / np.sqrt(dsq))
     else:
         gfac = dt.type(2) * gmain
+    gv = gfac[:, None] * d
+    if absolute:
+        e, gv = np.abs(e), np.abs(gv)
     np.add.at(E, bead, e)
-    np.add.at(G, bead, gfac[:, None] * d)
+    np.add.at(G, bead, gv)
     return E.reshape(shp), G.reshape(shp + (3,))
 
 

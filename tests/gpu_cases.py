@@ -71,13 +71,28 @@ def to_device_grid(case, device="cuda"):
                            keep_dense=True, device=device)
 
 
-def oracle_scales(case, poses, mode="reference", quirk=True):
-    """Per-pose magnitude scales for float32 tolerances: sum over beads of |E_b|
-    and of |dE/dx_b| * (1 + |r_b|)."""
+def oracle_scales(case, poses, mode="reference", quirk=True, position_term=False):
+    """Per-pose magnitude scales for float32 tolerances: the sum over every
+    grid corner and pair term of |energy term|, and of |gradient term| * (1 + |r_b|)
+    (float32 summation error is bounded relative to these, not to a total
+    in which large terms cancel).  ``position_term`` adds the float32 rounding
+    of the bead positions, |dE/dx| |x| ~1e-7, which dominates for steep
+    uncapped clashes."""
     G = case["G"]
     X = O.transform(poses, case["lig"])
-    Eb, gb = O.bead_energrad(X, case["gt"], case["lt"], G, mode, quirk)
+    absG = dict(G)
+    for k in ("inner", "outer"):
+        if k in G:
+            absG[k] = np.abs(G[k])
+    Eg, gg = O.grid_energrad(X, case["gt"], G["geom"], absG.get("inner"), absG.get("outer"), quirk, "reference")
+    En, gn = O.nb_energrad(X, case["lt"], G["geom"], G.get("nb_hdr"), G.get("nb_list"), G["rec"], G["rtype"],
+                           G["pair"], mode, absolute=True)
+    if mode == "analytic":  # the analytic grid gradient is bounded by |E corners| / spacing
+        gg = np.repeat(Eg[..., None], 3, -1) * 2.0 / G["geom"]["spacing"]
     r = X - poses[:, None, 3:6]
-    es = np.abs(Eb).sum(1)
-    gs = (np.linalg.norm(gb, axis=2) * (1 + np.linalg.norm(r, axis=2))).sum(1)
+    gabs = (np.abs(gg) + gn).sum(-1)
+    es = (Eg + En).sum(1)
+    if position_term:
+        es = es + 0.2 * (gabs * (1 + np.linalg.norm(X, axis=2))).sum(1)
+    gs = (gabs * (1 + np.linalg.norm(r, axis=2))).sum(1)
     return es, gs

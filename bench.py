@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the batched rigid-body minimiser (one JSON line on stdout).
+
+Workload (one "step"): the batched uneven-fragment minimisation -- a 2500-bead
+synthetic receptor, 6 fragments of 18/21/24/26/28/30 beads, 100 000 poses
+each (600 000 poses), 200 ADAM steps + a final evaluation, all fragments in
+one persistent, CUDA-graph-captured launch.  ``value`` = minimised poses/s with
+the inputs resident in HBM; ``e2e`` = the same through the public API with the
+poses copied from pinned host memory and the energies + poses copied back
+inside the timed region.  The 5.7 GB brick grid is larger than L2, so no L2
+flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun): every rank minimises its own copy of the workload (replicas,
+weak scaling); the time is the max over ranks.  ``--impl reference`` times the
+CPU restatement of the reference path (oracle/, NumPy) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "minimised poses/s/GPU (200 ADAM steps), batched+served vs plain; p99 latency"
+UNIT = "poses/s"
+WORKLOAD = ("config1 batched uneven: receptor 2500 beads (40 A sphere, 32 types), fragments of "
+            "18/21/24/26/28/30 beads x 100000 poses, 200 ADAM steps + final eval, fp32")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="pose-count scale (1 = the full workload)")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--cpu-poses", type=int, default=16, help="poses per fragment in the CPU sample")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling (200 ms) while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = np.array([float(r[1]) for r in rows])
+        mx = float(rows[0][2])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        load = sm[sm > 0.5 * sm.max()] if len(sm) else sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows),
+                "power_w_max": float(max(float(r[3]) for r in rows))}
+
+
+# --------------------------------------------------------------------------- workload
+def build(args, device):
+    import torch
+
+    import attract_b200 as A
+    from attract_b200 import synth
+
+    cfg = synth.make_config(1, seed=0, scale=args.scale)
+    grid = A.Grid.build(cfg.rec_xyz, cfg.rec_type, cfg.ff, cfg.geom, cutoff=cfg.cutoff, keep_dense=not args.no_cpu,
+                        device=device)
+    ligs = A.LigandSet(cfg.ligands, device=device)
+    order = sorted(range(len(cfg.ligands)), key=lambda i: -len(cfg.ligands[i][0]))  # largest first
+    segs = [A.Segment(0, i, len(cfg.poses[i])) for i in order]
+    poses = np.concatenate([cfg.poses[i] for i in order]).astype(np.float32)
+    return cfg, grid, ligs, segs, poses, order
+
+
+def algorithmic_bytes(stats):
+    """128 B per grid-brick read + 8 B per list header + 2 B per list entry."""
+    return int(stats[0]) * 128 + int(stats[1]) * 8 + int(stats[2]) * 2
+
+
+def plain_run(A, grid, cfg, order, poses_np, steps, device):
+    """The reference's call pattern on the GPU: one ligand at a time, one
+    energy+gradient launch per step, ADAM in torch ops on the host side."""
+    import torch
+
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    off = 0
+    launches = 0
+    t0.record()
+    for i in order:
+        n = len(cfg.poses[i])
+        wl = A.Workload([grid], A.LigandSet([cfg.ligands[i]], device=device), [A.Segment(0, 0, n)])
+        x = torch.tensor(poses_np[off:off + n], device=device)
+        off += n
+        m = torch.zeros_like(x)
+        v = torch.zeros_like(x)
+        lr = torch.tensor([cfg.lr_rot] * 3 + [cfg.lr_trans] * 3, device=device)
+        for s in range(1, steps + 1):
+            E, g, _ = A.energrad(wl, x)
+            launches += 1
+            m.mul_(0.9).add_(g, alpha=0.1)
+            v.mul_(0.999).addcmul_(g, g, value=0.001)
+            mh = m / (1 - 0.9 ** s)
+            vh = v / (1 - 0.999 ** s)
+            x = x - lr * mh / (vh.sqrt() + 1e-8)
+        E, _, _ = A.energrad(wl, x, grad=False)
+        launches += 1
+    t1.record()
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1) / 1e3, launches
+
+
+def cpu_baseline(cfg, grid, order, n_per_frag, steps):
+    """The oracle (NumPy float32, one process) on a bounded sample: the first
+    n_per_frag poses of every fragment, the full step count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import attract_oracle as O
+
+    inner, outer, hdr, lst = grid.dense_host()
+    G = dict(geom=cfg.geom.as_dict(), inner=inner, outer=outer, nb_hdr=hdr, nb_list=lst,
+             rec=np.asarray(cfg.rec_xyz, np.float32), rtype=cfg.rec_type,
+             pair=O.pair_table(cfg.ff.rc, cfg.ff.ac, cfg.ff.ivor, cfg.geom.plateau, True, cfg.ff.rcap2))
+    t = time.perf_counter()
+    n = 0
+    for i in order:
+        xyz, gt, lt = cfg.ligands[i]
+        p = cfg.poses[i][:n_per_frag]
+        O.minimise(p, np.asarray(xyz, np.float32), gt, lt, G, steps, cfg.lr_rot, cfg.lr_trans, dtype=np.float32)
+        n += len(p)
+    dt = time.perf_counter() - t
+    return {"value": n / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} poses ({n_per_frag} per fragment) x {steps} ADAM steps, NumPy float32 oracle, "
+                      f"1 process, {dt:.1f} s"}
+
+
+def traffic_from_profile(n_launch_units):
+    """DRAM bytes per launch from the committed ncu summary, scaled to this
+    launch by bead evaluations (the capture ran a smaller case)."""
+    path = os.path.join(ROOT, "profiles", "minimise_kernel_config1.txt")
+    if not os.path.exists(path):
+        return None
+    vals = {}
+    for line in open(path):
+        if "=" in line and line.strip().startswith("dram_bytes_per_bead_eval"):
+            vals["per"] = float(line.split("=")[1].split()[0])
+    if "per" not in vals:
+        return None
+    return vals["per"] * n_launch_units
+
+
+# --------------------------------------------------------------------------- ours
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+
+    import attract_b200 as A
+    from attract_b200.autotune import autotune
+
+    A.load_library()
+    cfg, grid, ligs, segs, poses_np, order = build(args, device)
+    steps = cfg.steps
+    wl = A.Workload([grid], ligs, segs)
+    poses = torch.tensor(poses_np, device=device)
+    tune_ms = {}
+    if args.lanes:
+        shape = A.LaunchShape(args.lanes, args.threads or 256)
+    elif args.no_autotune:
+        shape = A.LaunchShape()
+    else:
+        shape, tune_ms = autotune(wl, poses, use_cache=False)
+    wl = wl.with_lanes(shape.lanes_per_pose)
+
+    # statistics launch (untimed): bead evaluations, list lookups, entries
+    _, _, _, st = A.minimise(wl, poses, steps, launch=shape, stats=True)
+    stats = st.cpu().numpy()
+    alg_bytes = algorithmic_bytes(stats)
+
+    plan = A.MinimisePlan(wl, steps, launch=shape)
+    plan.pose_in.copy_(poses)
+    plan.capture()
+    for _ in range(args.warmup):
+        plan.replay()
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    if rank == 0:
+        clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        plan.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        ms = float(t.item())
+    E = plan.scratch.energy
+    status = plan.scratch.status
+    n_bad = int((status != 0).sum().item())
+
+    # e2e through the public API: pinned host poses in, energies + poses out
+    host_in = torch.from_numpy(poses_np).pin_memory()
+    host_E = torch.empty(wl.n_poses, dtype=torch.float32).pin_memory()
+    host_P = torch.empty((wl.n_poses, 6), dtype=torch.float32).pin_memory()
+    for _ in range(2):
+        plan.pose_in.copy_(host_in, non_blocking=True)
+        plan.replay()
+        host_E.copy_(plan.scratch.energy, non_blocking=True)
+        host_P.copy_(plan.pose_out, non_blocking=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(args.steps):
+        plan.pose_in.copy_(host_in, non_blocking=True)
+        plan.replay()
+        host_E.copy_(plan.scratch.energy, non_blocking=True)
+        host_P.copy_(plan.pose_out, non_blocking=True)
+    f1.record()
+    torch.cuda.synchronize()
+    ms_e2e = f0.elapsed_time(f1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    clk = clocks.stop() if rank == 0 else None
+
+    out = None
+    if rank == 0:
+        n_total = wl.n_poses * world
+        value = n_total / (ms / 1e3)
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+        peak = float(peaks.get("hbm_gbs", 6650.0))
+        achieved = alg_bytes / (ms / 1e3) / 1e9
+        bead_evals = int(stats[0])
+        traffic = traffic_from_profile(bead_evals)
+        out = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": WORKLOAD, "poses_per_step": wl.n_poses, "adam_steps": steps,
+                       "evals_per_pose": steps + 1, "l2": "inputs larger than L2 (brick grid "
+                       f"{grid.bricks.numel() * 4 / 1e9:.2f} GB, no flush needed)",
+                       "launch": {"lanes_per_pose": shape.lanes_per_pose, "block_threads": shape.block_threads},
+                       "autotune_ms": tune_ms, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "scale": args.scale},
+            "e2e": {"value": round(n_total / (ms_e2e / 1e3), 1), "unit": UNIT,
+                    "h2d_bytes_per_step": host_in.numel() * 4, "d2h_bytes_per_step": host_E.numel() * 4 +
+                    host_P.numel() * 4},
+            "gpu_launches": args.steps * 1,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg_bytes, "peak_source": "measured hbm_gbs",
+                         "counts": {"brick_reads": int(stats[0]), "list_lookups": int(stats[1]),
+                                    "list_entries": int(stats[2])}},
+            "clocks": clk,
+            "nonfinite_poses": n_bad,
+            "median_final_energy": float(E.median().item()),
+        }
+    if not args.no_plain and rank == 0:
+        dt, launches = plain_run(A, grid, cfg, order, poses_np, steps, device)
+        out["plain"] = {"value": round(wl.n_poses / dt, 1), "unit": UNIT, "seconds": round(dt, 3),
+                        "launches": launches, "note": "one ligand at a time, one energrad launch per step, "
+                                                      "ADAM in torch ops"}
+        out["batched_vs_plain"] = round(out["value"] / out["plain"]["value"], 2)
+    if not args.no_cpu and rank == 0 and world == 1:
+        out["cpu_baseline"] = cpu_baseline(cfg, grid, order, args.cpu_poses, steps)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# --------------------------------------------------------------------------- reference
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference_arm
+
+    out = reference_arm.run(args.steps, args.warmup, METRIC, UNIT, WORKLOAD, args.scale)
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -459,15 +459,19 @@ def grid_points(geom, outer=False):
     return np.stack(np.meshgrid(*ax, indexing="ij"), -1)
 
 
-def build_potential_grid(rec, rtype, pair_full, geom, n_types, cutoff, outer=False):
+def build_potential_grid(rec, rtype, pair_full, geom, n_types, cutoff, outer=False, point_range=None):
     """Energy + force voxels ``[n_types, dx, dy, dz, 4]`` for ligand types 0..n_types-1.
 
     Per receptor bead within ``cutoff``: beyond the plateau, E(d) and force
     -2 dnonbon d; inside it, the plateau energy and the plateau force along d
     (what the nbgrid term's plateau correction removes again, test5.py:220-229).
     ``pair_full`` must carry the plateau values (eplat, gplat) for ``geom``.
+    With ``point_range=(lo, hi)`` only those flat grid points are computed and
+    ``[n_types, hi-lo, 4]`` is returned (for building a large grid in chunks).
     """
     pts = grid_points(geom, outer).reshape(-1, 3)
+    lo, hi = (0, len(pts)) if point_range is None else point_range
+    pts = pts[lo:hi]
     rec = np.asarray(rec, np.float64)
     p = float(geom["plateau"])
     out = np.zeros((n_types, len(pts), 4))
@@ -490,9 +494,11 @@ def build_potential_grid(rec, rtype, pair_full, geom, n_types, cutoff, outer=Fal
         with np.errstate(divide="ignore", invalid="ignore"):
             scale = np.where(inside, np.where(dist > 0, gplat * p / dist, 0.0), g_far)
         f = -2.0 * scale[:, None] * d
-        np.add.at(out[lt, :, 0], gi, e)
+        out[lt, :, 0] = np.bincount(gi, e, minlength=len(pts))
         for k in range(3):
-            np.add.at(out[lt, :, 1 + k], gi, f[:, k])
+            out[lt, :, 1 + k] = np.bincount(gi, f[:, k], minlength=len(pts))
+    if point_range is not None:
+        return out
     d3 = geom["dim2"] if outer else geom["dim"]
     return out.reshape((n_types,) + tuple(int(x) for x in d3) + (4,))
 

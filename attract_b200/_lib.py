@@ -80,6 +80,7 @@ SIGNATURES = {
     "att_nbgrid_workspace_bytes": (LL, [LL]),
     "att_nbgrid_count": (I, [C.POINTER(AttGridGeom), P, I, F, P, P, P, LL, P]),
     "att_nbgrid_fill": (I, [C.POINTER(AttGridGeom), P, I, F, P, P, P]),
+    "att_kernel_status": (I, [C.POINTER(C.c_int), I, P]),
 }
 
 _lib = None
@@ -107,6 +108,16 @@ def check(rc: int, what: str = "") -> None:
     if rc != ATT_OK:
         msg = load().att_last_error_string().decode(errors="replace")
         raise AttractError(f"{what}: status {rc}: {msg}")
+
+
+def kernel_status(clear: bool = True, stream=None) -> int:
+    """The scoring kernels' device-wide error word (0 = no warp stopped early)."""
+    import torch
+
+    out = C.c_int(0)
+    st = torch.cuda.current_stream().cuda_stream if stream is None else stream
+    check(load().att_kernel_status(C.byref(out), int(clear), st), "att_kernel_status")
+    return out.value
 
 
 def ptr(t) -> int | None:

@@ -1,7 +1,7 @@
 """Launch-shape autotuner for the persistent minimiser.
 
 Candidates are (lanes per pose, threads per block): 8/16/32 lanes per pose
-(4/2/1 poses per warp) x 128/256 threads.  Each candidate minimises a sample
+(4/2/1 poses per warp) x 64/128 threads.  Each candidate minimises a sample
 of every segment for a few steps, timed with CUDA events; the fastest wins and
 is cached per (GPU, bead-count histogram) in a JSON file
 (``$ATTRACT_B200_CACHE`` or ``~/.cache/attract_b200/autotune.json``).
@@ -16,7 +16,7 @@ import torch
 
 from .engine import AdamOptions, EvalOptions, LaunchShape, Segment, Workload, minimise
 
-CANDIDATES = [(8, 128), (8, 256), (16, 128), (16, 256), (32, 128), (32, 256)]
+CANDIDATES = [(8, 64), (8, 128), (16, 64), (16, 128), (32, 64), (32, 128)]
 
 
 def _cache_path() -> str:

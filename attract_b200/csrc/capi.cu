@@ -6,8 +6,11 @@
 #include "common.cuh"
 
 namespace att {
-cudaError_t launch_score(const KParams& p, int mode, int S, int blocks, int threads, cudaStream_t st);
-cudaError_t occupancy_blocks(int mode, int S, int threads, int* blocks_per_sm);
+cudaError_t launch_score(const KParams& p, int mode, int S, int K, int blocks, int threads, cudaStream_t st);
+cudaError_t occupancy_blocks(int mode, int S, int K, int threads, int* blocks_per_sm);
+cudaError_t kernel_status(int* out, int clear, cudaStream_t st);
+int beads_per_lane(int S, int max_beads);
+size_t score_smem_bytes(int K, int threads);
 cudaError_t launch_build_potential(const AttGridGeom& g, const float* rec, int n_rec, const float* pair,
                                    int n_rtypes, int n_ltypes, float cutoff, int outer, float* out,
                                    cudaStream_t st);
@@ -128,7 +131,8 @@ static int make_kgrid(const AttGrid* a, int gi, KGrid* k) {
 
 static int fill_common(KParams* p, const AttGrid* grids, int n_grids, const AttLigands* ligs,
                        const AttSegment* segs, int n_segs, const int* seg_tile, int n_tiles, const float* pose,
-                       const int* pose_lig, const AttEvalCfg* cfg, const AttLaunchCfg* launch, int* S) {
+                       const int* pose_lig, const AttEvalCfg* cfg, const AttLaunchCfg* launch, int* S, int* K,
+                       int* threads) {
   REQUIRE(grids != nullptr && n_grids >= 1 && n_grids <= ATT_MAX_GRIDS, "n_grids = %d out of range [1, %d]",
           n_grids, ATT_MAX_GRIDS);
   REQUIRE(ligs != nullptr && ligs->beads != nullptr && ligs->offset != nullptr && ligs->n_lig >= 1,
@@ -143,6 +147,13 @@ static int fill_common(KParams* p, const AttGrid* grids, int n_grids, const AttL
   int s = (launch && launch->lanes_per_pose) ? launch->lanes_per_pose : 8;
   REQUIRE(s == 8 || s == 16 || s == 32, "lanes_per_pose = %d (8, 16 or 32)", s);
   *S = s;
+  REQUIRE(ligs->max_beads >= 1, "ligands: max_beads = %d", ligs->max_beads);
+  *K = beads_per_lane(s, ligs->max_beads);
+  const int t = (launch && launch->block_threads) ? launch->block_threads : 128;
+  REQUIRE(t == 32 || t == 64 || t == 96 || t == 128, "block_threads = %d (32, 64, 96 or 128)", t);
+  REQUIRE(score_smem_bytes(*K, t) <= 227 * 1024, "%d threads x %d beads per lane need %zu B of shared memory", t,
+          *K, score_smem_bytes(*K, t));
+  *threads = t;
   memset(p, 0, sizeof(*p));
   for (int i = 0; i < n_grids; ++i) {
     int rc = make_kgrid(&grids[i], i, &p->grid[i]);
@@ -162,38 +173,30 @@ static int fill_common(KParams* p, const AttGrid* grids, int n_grids, const AttL
   return ATT_OK;
 }
 
-static int threads_of(const AttLaunchCfg* launch) {
-  int t = (launch && launch->block_threads) ? launch->block_threads : 256;
-  return t;
-}
-
 extern "C" int att_energrad(const AttGrid* grids, int n_grids, const AttLigands* ligs, const AttSegment* segs_dev,
                             int n_segs, const int* seg_tile_dev, int n_tiles, const float* pose_dev,
                             const int* pose_lig_dev, const AttEvalCfg* cfg, float* energy_dev, float* grad_dev,
                             int* status_dev, const AttLaunchCfg* launch, void* stream) {
   KParams p;
-  int S = 8;
+  int S = 8, K = 1, threads = 128;
   int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, pose_dev, pose_lig_dev,
-                       cfg, launch, &S);
+                       cfg, launch, &S, &K, &threads);
   if (rc) return rc;
   REQUIRE(energy_dev != nullptr || n_tiles == 0, "energy output is NULL");
   REQUIRE(cfg->pose_format == 0 || cfg->pose_format == 1, "pose_format %d unknown", cfg->pose_format);
-  const int threads = threads_of(launch);
-  REQUIRE(threads % 32 == 0 && threads >= 32 && threads <= 256, "block_threads = %d (multiple of 32, <= 256)",
-          threads);
   p.energy = energy_dev;
   p.grad = grad_dev;
   p.status = status_dev;
   if (n_tiles == 0) return ATT_OK;
   const int wpb = threads / 32;
   const int blocks = (n_tiles + wpb - 1) / wpb;
-  cudaError_t e = launch_score(p, cfg->pose_format == 1 ? MODE_EVAL_MAT : MODE_EVAL, S, blocks, threads,
+  cudaError_t e = launch_score(p, cfg->pose_format == 1 ? MODE_EVAL_MAT : MODE_EVAL, S, K, blocks, threads,
                                (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(e, "att_energrad launch");
   return ATT_OK;
 }
 
-static int persistent_blocks(int mode, int S, int threads, const AttLaunchCfg* launch, int n_tiles, int* blocks) {
+static int persistent_blocks(int mode, int S, int K, int threads, const AttLaunchCfg* launch, int n_tiles, int* blocks) {
   if (launch && launch->blocks > 0) {
     *blocks = launch->blocks;
     return ATT_OK;
@@ -201,7 +204,7 @@ static int persistent_blocks(int mode, int S, int threads, const AttLaunchCfg* l
   int dev = 0, sms = 0, per = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess) e = occupancy_blocks(mode, S, threads, &per);
+  if (e == cudaSuccess) e = occupancy_blocks(mode, S, K, threads, &per);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   if (per < 1) per = 1;
   const int wpb = threads / 32;
@@ -221,9 +224,9 @@ extern "C" int att_minimise(const AttGrid* grids, int n_grids, const AttLigands*
                             void* stream) {
   REQUIRE(cfg != nullptr, "adam cfg is NULL");
   KParams p;
-  int S = 8;
+  int S = 8, K = 1, threads = 128;
   int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, pose_in_dev,
-                       pose_lig_dev, &cfg->eval, launch, &S);
+                       pose_lig_dev, &cfg->eval, launch, &S, &K, &threads);
   if (rc) return rc;
   REQUIRE(cfg->eval.pose_format == 0, "att_minimise takes Euler poses (pose_format 0)");
   REQUIRE(steps >= 0, "steps = %d < 0", steps);
@@ -233,9 +236,6 @@ extern "C" int att_minimise(const AttGrid* grids, int n_grids, const AttLigands*
   REQUIRE(cfg->beta1 >= 0.f && cfg->beta1 < 1.f && cfg->beta2 >= 0.f && cfg->beta2 < 1.f,
           "beta1/beta2 must be in [0, 1)");
   REQUIRE(cfg->step0 >= 0, "step0 < 0");
-  const int threads = threads_of(launch);
-  REQUIRE(threads % 32 == 0 && threads >= 32 && threads <= 256, "block_threads = %d (multiple of 32, <= 256)",
-          threads);
   p.pose_out = pose_out_dev;
   p.adam = adam_state_dev;
   p.energy = energy_dev;
@@ -251,12 +251,12 @@ extern "C" int att_minimise(const AttGrid* grids, int n_grids, const AttLigands*
   p.step0 = cfg->step0;
   if (n_tiles == 0) return ATT_OK;
   int blocks = 0;
-  rc = persistent_blocks(MODE_MIN, S, threads, launch, n_tiles, &blocks);
+  rc = persistent_blocks(MODE_MIN, S, K, threads, launch, n_tiles, &blocks);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e = cudaMemsetAsync(work_counter_dev, 0, sizeof(int), st);
   if (e != cudaSuccess) return cuda_fail(e, "att_minimise counter reset");
-  e = launch_score(p, MODE_MIN, S, blocks, threads, st);
+  e = launch_score(p, MODE_MIN, S, K, blocks, threads, st);
   if (e != cudaSuccess) return cuda_fail(e, "att_minimise launch");
   return ATT_OK;
 }
@@ -267,15 +267,12 @@ extern "C" int att_energrad_backward(const AttGrid* grids, int n_grids, const At
                                      const float* dL_dE_dev, float* dL_dpose_dev, float* dgrid_inner_dev,
                                      float* dgrid_outer_dev, const AttLaunchCfg* launch, void* stream) {
   KParams p;
-  int S = 8;
+  int S = 8, K = 1, threads = 128;
   int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, pose_dev, pose_lig_dev,
-                       cfg, launch, &S);
+                       cfg, launch, &S, &K, &threads);
   if (rc) return rc;
   REQUIRE(cfg->pose_format == 0, "att_energrad_backward takes Euler poses (pose_format 0)");
   REQUIRE(dL_dE_dev != nullptr || n_tiles == 0, "dL_dE is NULL");
-  const int threads = threads_of(launch);
-  REQUIRE(threads % 32 == 0 && threads >= 32 && threads <= 256, "block_threads = %d (multiple of 32, <= 256)",
-          threads);
   p.dLdE = dL_dE_dev;
   p.dLdpose = dL_dpose_dev;
   p.dgrid_inner = dgrid_inner_dev;
@@ -283,7 +280,7 @@ extern "C" int att_energrad_backward(const AttGrid* grids, int n_grids, const At
   if (n_tiles == 0) return ATT_OK;
   const int wpb = threads / 32;
   const int blocks = (n_tiles + wpb - 1) / wpb;
-  cudaError_t e = launch_score(p, MODE_BWD, S, blocks, threads, (cudaStream_t)stream);
+  cudaError_t e = launch_score(p, MODE_BWD, S, K, blocks, threads, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(e, "att_energrad_backward launch");
   return ATT_OK;
 }
@@ -317,6 +314,13 @@ extern "C" int att_build_potential_grid(const AttGridGeom* geom, const float* re
   cudaError_t e = launch_build_potential(*geom, rec_dev, n_rec, pair_dev, n_rtypes, n_ltypes, cutoff, outer,
                                          out_dev, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(e, "att_build_potential_grid");
+  return ATT_OK;
+}
+
+extern "C" int att_kernel_status(int* error_word, int clear, void* stream) {
+  REQUIRE(error_word != nullptr, "error_word is NULL");
+  cudaError_t e = kernel_status(error_word, clear, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "att_kernel_status");
   return ATT_OK;
 }
 

@@ -1,17 +1,29 @@
 // Scoring and fused minimisation kernels (K1 energrad / minimise, K2 adjoint).
 //
-// One pose is served by a team of S lanes (S = 8, 16 or 32; 32/S poses per
-// warp).  A team is split into 8-lane subteams; a subteam takes one ligand bead
-// at a time and its 8 lanes cooperate on it:
-//   * lane c reads trilinear corner c of the bead's 128-byte grid brick (the 8
-//     corners are contiguous, so the subteam issues one coalesced 128-B load),
-//   * the lanes stride over the bead's neighbour list (entry c, c+8, ...).
-// Energy, dE/dx and the torque are linear in the per-corner / per-pair
-// contributions, so every lane accumulates its own share and the team sums its
-// 7 accumulators with xor-shuffles once per step.  The rigid-body ADAM update
-// of the 6 pose DOFs runs on team lanes 0..5 between steps, the pose never
-// leaves registers, and a persistent launch pulls tiles of poses from a work
-// counter until all segments are done.
+// A pose is served by a team of S lanes (S = 8, 16 or 32: 32/S poses per warp).
+// Team lane l owns ligand beads l, l+S, ... (K beads per lane, N <= K*S); the
+// ligand-frame coordinates stay in registers for the whole minimisation.  One
+// evaluation of a pose runs in four phases:
+//
+//  A  every owner lane moves its beads, computes the voxel, and starts a
+//     128-byte bulk copy (TMA engine, cp.async.bulk) of the bead's grid brick --
+//     the 8 trilinear corners of the voxel, (E, Fx, Fy, Fz) each -- into its
+//     shared-memory slot, completing on the warp's mbarrier; it also loads the
+//     bead's neighbour-list header {start, count};
+//  B  a team scan of the list lengths gives every bead's offset in the team's
+//     flattened list of (bead, entry) pairs;
+//  C  the team walks that flattened list, each lane a contiguous chunk, with all
+//     list-entry loads of a chunk issued before the receptor loads and the pair
+//     math -- so the bricks stream in while the pair terms are computed;
+//  D  after the mbarrier completes, each owner reads its brick from shared
+//     memory (rotated chunk order: conflict-free) and adds the grid term.
+//
+// Energy, dE/dt and the torque are linear in every corner / pair contribution,
+// so each lane accumulates its own share and the team sums 7 values with
+// xor-shuffles per evaluation.  The rigid-body ADAM step runs on team lanes
+// 0..5 between evaluations; a persistent launch pulls tiles of poses from a
+// work counter.  Every mbarrier wait is bounded; a timeout sets an error word
+// and the warp returns.
 //
 // Semantics follow test5.py (sjdv1982/attract-jax):
 //   transform            [x,1] @ mat                    test5.py:315-317
@@ -28,117 +40,69 @@
 
 namespace att {
 
-struct BeadAcc {
-  float e, gx, gy, gz;   // energy and dE/dx of this lane's share
+// ---------------------------------------------------------------------------
+// shared memory / mbarrier / bulk-copy helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}"
+               ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// 128-byte brick: global -> shared through the bulk-copy (TMA) engine
+__device__ __forceinline__ void bulk_brick(void* dst, const void* src, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 128, [%2];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// per-bead records shared by the team
+struct __align__(16) BeadPos {  // moved bead; w = ligand type (int bits)
+  float x, y, z;
+  int lt;
+};
+struct __align__(16) BeadArm {  // lever arm for the torque (Q x) or ligand-frame x (dE/dmat)
+  float x, y, z, pad;
+};
+struct __align__(16) BeadList {  // neighbour list: start, count, offset in the flattened team list
+  unsigned start, count, pre, pad;
 };
 
-template <int MODE>
-struct PoseAcc {
-  // energy, dE/dt, then torque (3) or dE/dmat rows (9)
-  static constexpr int NT = (MODE == MODE_EVAL_MAT) ? 9 : 3;
-  float e, gx, gy, gz;
-  float t[NT];
-};
+constexpr int WAIT_LIMIT = 1 << 22;  // try_wait polls before a bulk-copy wait is declared hung
 
-// Per-bead work of one subteam lane: grid corner `corner` and list entries
-// corner, corner+8, ...  X is the moved bead, (bx,by,bz) its ligand-frame
-// coordinates.  `dscale` scales scatter-added grid gradients (MODE_BWD).
-template <int MODE>
-__device__ __forceinline__ void bead_work(const KParams& p, const KGrid& G, int corner, float X, float Y,
-                                          float Z, int gt, int lt, BeadAcc& a, float dscale,
-                                          unsigned& c_grid, unsigned& c_look, unsigned& c_ent) {
-  const float vx = (X - G.ox) * G.inv_s;
-  const float vy = (Y - G.oy) * G.inv_s;
-  const float vz = (Z - G.oz) * G.inv_s;
-  const bool inn = (vx >= 0.f) & (vx < G.fdx1) & (vy >= 0.f) & (vy < G.fdy1) & (vz >= 0.f) & (vz < G.fdz1);
-  if (G.bricks != nullptr && gt < G.n_types) {
-    float ux = vx, uy = vy, uz = vz, scale = G.inv_s;
-    bool use = inn;
-    int ny = G.dy, nz = G.dz;
-    long long base = 0;
-    if (!inn && G.has_outer) {
-      ux = (vx + G.ext) * 0.5f;
-      uy = (vy + G.ext) * 0.5f;
-      uz = (vz + G.ext) * 0.5f;
-      use = (ux >= 0.f) & (ux < G.fex1) & (uy >= 0.f) & (uy < G.fey1) & (uz >= 0.f) & (uz < G.fez1);
-      scale = 0.5f * G.inv_s;
-      ny = G.dy2;
-      nz = G.dz2;
-      base = G.n_inner;
-    }
-    if (use) {
-      const float flx = floorf(ux), fly = floorf(uy), flz = floorf(uz);
-      const float fx = ux - flx, fy = uy - fly, fz = uz - flz;
-      // reference floor/ceil weights vanish on an exactly integer coordinate
-      if (p.quirk && ((fx == 0.f) | (fy == 0.f) | (fz == 0.f))) use = false;
-      if (use) {
-        const int ix = (int)flx, iy = (int)fly, iz = (int)flz;
-        const long long brick = (long long)gt * G.type_stride + base +
-                                ((long long)ix * (ny - 1) + iy) * (nz - 1) + iz;
-        const float4 c = ldg_stream_f4(G.bricks + brick * 8 + corner);
-        const int cx = (corner >> 2) & 1, cy = (corner >> 1) & 1, cz = corner & 1;
-        const float wx = cx ? fx : 1.f - fx;
-        const float wy = cy ? fy : 1.f - fy;
-        const float wz = cz ? fz : 1.f - fz;
-        const float w = wx * wy * wz;
-        a.e = fmaf(w, c.x, a.e);
-        if (p.grad_mode == ATT_GRAD_REFERENCE) {
-          a.gx = fmaf(-w, c.y, a.gx);
-          a.gy = fmaf(-w, c.z, a.gy);
-          a.gz = fmaf(-w, c.w, a.gz);
-        } else {
-          const float ce = c.x * scale;
-          a.gx = fmaf(ce, (cx ? 1.f : -1.f) * wy * wz, a.gx);
-          a.gy = fmaf(ce, wx * (cy ? 1.f : -1.f) * wz, a.gy);
-          a.gz = fmaf(ce, wx * wy * (cz ? 1.f : -1.f), a.gz);
-        }
-        if (MODE == MODE_BWD) {
-          float* dg = base ? p.dgrid_outer : p.dgrid_inner;
-          if (dg != nullptr) {
-            const int gx = ix + cx, gy = iy + cy, gz = iz + cz;
-            const int nx = base ? G.dx2 : G.dx;
-            const long long off = ((((long long)gt * nx + gx) * ny + gy) * (long long)nz + gz) * 4;
-            atomicAdd(dg + off, dscale * w);
-          }
-        }
-        if (MODE == MODE_MIN && corner == 0) c_grid += 1;
-      }
-    }
-  }
-  if (G.nb_hdr != nullptr && inn && lt < G.n_ltypes) {
-    const int nx = (int)floorf(vx + 0.5f), ny = (int)floorf(vy + 0.5f), nz = (int)floorf(vz + 0.5f);
-    const uint2 h = ldg_u2(G.nb_hdr + (((long long)nx * G.dy + ny) * G.dz + nz));
-    if (MODE == MODE_MIN && corner == 0) c_look += 1;
-    const float4* prow = G.pair + (long long)lt * G.n_rtypes * 2;
-    for (unsigned e = corner; e < h.y; e += 8) {
-      const unsigned j = ldg_u16(G.nb_list + h.x + e);
-      if (MODE == MODE_MIN) c_ent += 1;
-      if (j >= (unsigned)G.n_rec) continue;  // ATT_NB_EMPTY and corrupt entries
-      const float4 r = ldg_f4(G.rec + j);
-      const float dx = X - r.x, dy = Y - r.y, dz = Z - r.z;
-      const float dsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      if (!(dsq < G.plateau2)) continue;
-      const int rt = __float_as_int(r.w);
-      if ((unsigned)rt >= (unsigned)G.n_rtypes) continue;
-      const float4 p0 = ldg_f4(prow + rt * 2);      // rc, ac, emin, rmin2
-      const float4 p1 = ldg_f4(prow + rt * 2 + 1);  // ivor, eplat, gplat, rcap2
-      const float d2 = fmaxf(dsq, p1.w);
-      const float rr2 = __frcp_rn(d2);
-      const float rr6 = rr2 * rr2 * rr2;
-      const float vlj = fmaf(p0.x, rr2, -p0.y) * rr6;
-      const bool near = d2 < p0.w;
-      const float en = near ? fmaf(p1.x - 1.f, p0.z, vlj) : p1.x * vlj;
-      const float dv = rr6 * rr2 * fmaf(-4.f * p0.x, rr2, 3.f * p0.y);
-      float gm = near ? dv : p1.x * dv;
-      if (dsq < p1.w) gm = 0.f;
-      a.e += en - p1.y;
-      if (p.grad_mode == ATT_GRAD_REFERENCE) gm = fmaf(-p1.z * G.plateau, rsqrtf(dsq), gm);
-      const float gf = 2.f * gm;
-      a.gx = fmaf(gf, dx, a.gx);
-      a.gy = fmaf(gf, dy, a.gy);
-      a.gz = fmaf(gf, dz, a.gz);
-    }
-  }
+// device-wide error word of the scoring kernels (ATT_KERR_* bits), read and
+// cleared by att_kernel_status()
+__device__ int g_kernel_error = 0;
+
+template <int K>
+__host__ __device__ constexpr size_t warp_smem_bytes() {
+  return (size_t)32 * K * (128 + sizeof(BeadPos) + sizeof(BeadArm) + sizeof(BeadList)) + 16;
 }
 
 template <int S>
@@ -157,28 +121,72 @@ __device__ __forceinline__ int find_segment(const KParams& p, int tile) {
   return lo;
 }
 
-template <int S, int MODE>
-__global__ void __launch_bounds__(256) score_kernel(const __grid_constant__ KParams p) {
-  constexpr int P = 32 / S;
-  constexpr int NSUB = S / 8;
+// pair term of one (bead, receptor bead) entry; adds to e and returns dE/dx in g
+__device__ __forceinline__ void pair_term(const KParams& p, const KGrid& G, const BeadPos& bp, const float4& r,
+                                          float& e, float& gx, float& gy, float& gz, bool& hit) {
+  const float dx = bp.x - r.x, dy = bp.y - r.y, dz = bp.z - r.z;
+  const float dsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const int rt = __float_as_int(r.w);
+  hit = (dsq < G.plateau2) && ((unsigned)rt < (unsigned)G.n_rtypes) && ((unsigned)bp.lt < (unsigned)G.n_ltypes);
+  if (!hit) return;
+  const float4* pp = G.pair + ((long long)bp.lt * G.n_rtypes + rt) * 2;
+  const float4 p0 = ldg_f4(pp);      // rc, ac, emin, rmin2
+  const float4 p1 = ldg_f4(pp + 1);  // ivor, eplat, gplat, rcap2
+  const float d2 = fmaxf(dsq, p1.w);
+  const float rr2 = __frcp_rn(d2);
+  const float rr6 = rr2 * rr2 * rr2;
+  const float vlj = fmaf(p0.x, rr2, -p0.y) * rr6;
+  const bool near = d2 < p0.w;
+  const float en = near ? fmaf(p1.x - 1.f, p0.z, vlj) : p1.x * vlj;
+  const float dv = rr6 * rr2 * fmaf(-4.f * p0.x, rr2, 3.f * p0.y);
+  float gm = near ? dv : p1.x * dv;
+  if (dsq < p1.w) gm = 0.f;
+  e += en - p1.y;
+  if (p.grad_mode == ATT_GRAD_REFERENCE) gm = fmaf(-p1.z * G.plateau, rsqrtf(dsq), gm);
+  const float gf = 2.f * gm;
+  gx = gf * dx;
+  gy = gf * dy;
+  gz = gf * dz;
+}
+
+template <int S, int K, int MODE>
+__global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KParams p) {
+  constexpr int P = 32 / S;      // poses per warp
+  constexpr int NB = S * K;      // bead slots per pose
+  constexpr int U = 8;           // list entries in flight per lane
+  constexpr bool MAT = (MODE == MODE_EVAL_MAT);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+
   const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   const int slot = lane / S;
   const int tl = lane % S;
-  const int sub = tl >> 3;
-  const int corner = lane & 7;
-  const int lead = slot * S;  // team lane 0
+  const int lead = slot * S;
+  unsigned char* wsm = smem_raw + (size_t)warp * warp_smem_bytes<K>();
+  float4* bricks = reinterpret_cast<float4*>(wsm);                          // [32K][8]
+  BeadPos* bpos = reinterpret_cast<BeadPos*>(wsm + 32 * K * 128);
+  BeadArm* barm = reinterpret_cast<BeadArm*>(wsm + 32 * K * (128 + 16));
+  BeadList* blst = reinterpret_cast<BeadList*>(wsm + 32 * K * (128 + 32));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + 32 * K * (128 + 48));
+  const int tbase = slot * NB;  // this team's first bead record
+
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  uint32_t parity = 0;
 
   unsigned c_grid = 0, c_look = 0, c_ent = 0;  // statistics (MODE_MIN)
 
   int tile;
-  const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   if (p.counter != nullptr) {
     int t0 = 0;
     if (lane == 0) t0 = atomicAdd(p.counter, 1);
     tile = __shfl_sync(0xffffffffu, t0, 0);
   } else {
-    tile = warp_global;
+    tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   }
 
   while (tile < p.n_tiles) {
@@ -191,21 +199,43 @@ __global__ void __launch_bounds__(256) score_kernel(const __grid_constant__ KPar
     int lig = sg.lig;
     if (p.pose_lig != nullptr && valid) lig += __ldg(p.pose_lig + b);
     const int loff = __ldg(p.lig_off + lig);
-    const int N = valid ? __ldg(p.lig_off + lig + 1) - loff : 0;
+    const int Ntot = valid ? __ldg(p.lig_off + lig + 1) - loff : 0;
+    // ligands larger than the team's NB bead slots are evaluated in chunks of
+    // NB beads; the chunk count is warp-uniform (the mbarrier is per warp)
+    const int nchunk = __reduce_max_sync(0xffffffffu, (unsigned)((Ntot + NB - 1) / NB));
+    const bool multi = nchunk > 1;
 
-    // ---- pose state: team lane k < 6 owns DOF k ----
+    // owned ligand beads (ligand frame), resident for the whole tile
+    float lx[K], ly[K], lz[K];
+    int ltw[K];
+    auto load_beads = [&](int c0) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int i = c0 + tl + k * S;
+        if (i < Ntot) {
+          const float4 bd = ldg_f4(p.lig_beads + loff + i);
+          lx[k] = bd.x; ly[k] = bd.y; lz[k] = bd.z;
+          ltw[k] = __float_as_int(bd.w);
+        } else {
+          lx[k] = ly[k] = lz[k] = 0.f;
+          ltw[k] = -1;
+        }
+      }
+    };
+    load_beads(0);
+
+    // pose state: team lane k < 6 owns DOF k
     float my_x = 0.f, my_m = 0.f, my_v = 0.f;
     float mat[12];
-    if (MODE == MODE_EVAL_MAT) {
+    if (MAT) {
 #pragma unroll
-      for (int k = 0; k < 12; ++k) mat[k] = valid ? __ldg(p.pose_in + (long long)b * 16 + (k / 3) * 4 + (k % 3)) : 0.f;
-    } else {
-      if (valid && tl < 6) {
-        my_x = __ldg(p.pose_in + (long long)b * 6 + tl);
-        if (MODE == MODE_MIN && p.adam != nullptr) {
-          my_m = p.adam[(long long)b * 12 + tl];
-          my_v = p.adam[(long long)b * 12 + 6 + tl];
-        }
+      for (int k = 0; k < 12; ++k)
+        mat[k] = valid ? __ldg(p.pose_in + (long long)b * 16 + (k / 3) * 4 + (k % 3)) : 0.f;
+    } else if (valid && tl < 6) {
+      my_x = __ldg(p.pose_in + (long long)b * 6 + tl);
+      if (MODE == MODE_MIN && p.adam != nullptr) {
+        my_m = p.adam[(long long)b * 12 + tl];
+        my_v = p.adam[(long long)b * 12 + 6 + tl];
       }
     }
     const float dLdE = (MODE == MODE_BWD && valid) ? __ldg(p.dLdE + b) : 0.f;
@@ -213,10 +243,10 @@ __global__ void __launch_bounds__(256) score_kernel(const __grid_constant__ KPar
     const int nsteps = (MODE == MODE_MIN) ? p.steps : 0;
 
     for (int s = 0; s <= nsteps; ++s) {
+      // ---------------- pose -> rotation Q (column form) and translation t
       float q00, q01, q02, q10, q11, q12, q20, q21, q22, tx, ty, tz;
       float sphi = 0.f, cphi = 1.f, spsi = 0.f, cpsi = 1.f;
-      if (MODE == MODE_EVAL_MAT) {
-        // x'_j = sum_i x_i mat[i][j] + mat[3][j]  ->  Q[j][i] = mat[i][j]
+      if (MAT) {
         q00 = mat[0]; q10 = mat[1]; q20 = mat[2];
         q01 = mat[3]; q11 = mat[4]; q21 = mat[5];
         q02 = mat[6]; q12 = mat[7]; q22 = mat[8];
@@ -244,52 +274,283 @@ __global__ void __launch_bounds__(256) score_kernel(const __grid_constant__ KPar
         q22 = cpsi;
       }
 
-      PoseAcc<MODE> acc;
-      acc.e = acc.gx = acc.gy = acc.gz = 0.f;
+      float acc_e = 0.f, acc_gx = 0.f, acc_gy = 0.f, acc_gz = 0.f;
+      float acc_t[MAT ? 9 : 3];
 #pragma unroll
-      for (int k = 0; k < PoseAcc<MODE>::NT; ++k) acc.t[k] = 0.f;
+      for (int k = 0; k < (MAT ? 9 : 3); ++k) acc_t[k] = 0.f;
 
-      for (int i = sub; i < N; i += NSUB) {
-        const float4 bd = ldg_f4(p.lig_beads + loff + i);
-        const int tw = __float_as_int(bd.w);
-        const int gt = tw & 0xffff, lt = (tw >> 16) & 0xffff;
-        const float rx = fmaf(q00, bd.x, fmaf(q01, bd.y, q02 * bd.z));
-        const float ry = fmaf(q10, bd.x, fmaf(q11, bd.y, q12 * bd.z));
-        const float rz = fmaf(q20, bd.x, fmaf(q21, bd.y, q22 * bd.z));
-        BeadAcc a = {0.f, 0.f, 0.f, 0.f};
-        bead_work<MODE>(p, G, corner, rx + tx, ry + ty, rz + tz, gt, lt, a, dLdE, c_grid, c_look, c_ent);
-        acc.e += a.e;
-        acc.gx += a.gx;
-        acc.gy += a.gy;
-        acc.gz += a.gz;
-        if (MODE == MODE_EVAL_MAT) {
-          // dE/dmat[i][j] = sum_b x_b,i g_b,j
-          acc.t[0] = fmaf(bd.x, a.gx, acc.t[0]);
-          acc.t[1] = fmaf(bd.x, a.gy, acc.t[1]);
-          acc.t[2] = fmaf(bd.x, a.gz, acc.t[2]);
-          acc.t[3] = fmaf(bd.y, a.gx, acc.t[3]);
-          acc.t[4] = fmaf(bd.y, a.gy, acc.t[4]);
-          acc.t[5] = fmaf(bd.y, a.gz, acc.t[5]);
-          acc.t[6] = fmaf(bd.z, a.gx, acc.t[6]);
-          acc.t[7] = fmaf(bd.z, a.gy, acc.t[7]);
-          acc.t[8] = fmaf(bd.z, a.gz, acc.t[8]);
-        } else {
-          // torque r x g with r = Q x
-          acc.t[0] = fmaf(ry, a.gz, fmaf(-rz, a.gy, acc.t[0]));
-          acc.t[1] = fmaf(rz, a.gx, fmaf(-rx, a.gz, acc.t[1]));
-          acc.t[2] = fmaf(rx, a.gy, fmaf(-ry, a.gx, acc.t[2]));
+      for (int chunk = 0; chunk < nchunk; ++chunk) {
+      const int c0 = chunk * NB;
+      const int N = max(0, min(Ntot - c0, NB));  // beads of this chunk
+      if (multi) load_beads(c0);
+      // ---------------- phase A: move beads, start brick copies, list headers
+      float fx[K], fy[K], fz[K], gscale[K];
+      int brick_gt[K], bix[K], biy[K], biz[K];  // grid slot, base voxel (for the adjoint scatter)
+      bool use[K], outer_k[K];
+      long long bidx[K];  // brick index
+      long long nvox[K];  // nearest inner grid point for the list lookup, -1 = none
+      uint2 hdr[K];
+      unsigned nuse = 0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int i = tl + k * S;
+        const bool live = i < N;
+        const float rx = fmaf(q00, lx[k], fmaf(q01, ly[k], q02 * lz[k]));
+        const float ry = fmaf(q10, lx[k], fmaf(q11, ly[k], q12 * lz[k]));
+        const float rz = fmaf(q20, lx[k], fmaf(q21, ly[k], q22 * lz[k]));
+        const float X = rx + tx, Y = ry + ty, Z = rz + tz;
+        const int gt = ltw[k] & 0xffff, lt = (ltw[k] >> 16) & 0xffff;
+        const float vx = (X - G.ox) * G.inv_s;
+        const float vy = (Y - G.oy) * G.inv_s;
+        const float vz = (Z - G.oz) * G.inv_s;
+        const bool inn = live & (vx >= 0.f) & (vx < G.fdx1) & (vy >= 0.f) & (vy < G.fdy1) & (vz >= 0.f) &
+                         (vz < G.fdz1);
+        bool u = false;
+        float ux = vx, uy = vy, uz = vz;
+        float sc = G.inv_s;
+        int ny = G.dy, nz = G.dz;
+        long long base = 0;
+        outer_k[k] = false;
+        if (live && G.bricks != nullptr && gt < G.n_types) {
+          u = inn;
+          if (!inn && G.has_outer) {
+            ux = (vx + G.ext) * 0.5f;
+            uy = (vy + G.ext) * 0.5f;
+            uz = (vz + G.ext) * 0.5f;
+            u = (ux >= 0.f) & (ux < G.fex1) & (uy >= 0.f) & (uy < G.fey1) & (uz >= 0.f) & (uz < G.fez1);
+            sc = 0.5f * G.inv_s;
+            ny = G.dy2;
+            nz = G.dz2;
+            base = G.n_inner;
+            outer_k[k] = true;
+          }
+        }
+        const float flx = floorf(ux), fly = floorf(uy), flz = floorf(uz);
+        fx[k] = ux - flx;
+        fy[k] = uy - fly;
+        fz[k] = uz - flz;
+        gscale[k] = sc;
+        // reference floor/ceil weights vanish on an exactly integer coordinate
+        if (u && p.quirk && ((fx[k] == 0.f) | (fy[k] == 0.f) | (fz[k] == 0.f))) u = false;
+        use[k] = u;
+        brick_gt[k] = gt;
+        bix[k] = (int)flx;
+        biy[k] = (int)fly;
+        biz[k] = (int)flz;
+        bidx[k] = u ? (long long)gt * G.type_stride + base + ((long long)bix[k] * (ny - 1) + biy[k]) * (nz - 1) +
+                          biz[k]
+                    : 0;
+        nvox[k] = -1;
+        if (inn && G.nb_hdr != nullptr && lt < G.n_ltypes) {
+          const int nx = (int)floorf(vx + 0.5f), my = (int)floorf(vy + 0.5f), mz = (int)floorf(vz + 0.5f);
+          nvox[k] = ((long long)nx * G.dy + my) * G.dz + mz;
+        }
+        nuse += __popc(__ballot_sync(0xffffffffu, u));
+        // records for the team (generic-proxy writes)
+        if (live) {
+          BeadPos bp;
+          bp.x = X; bp.y = Y; bp.z = Z; bp.lt = lt;
+          bpos[tbase + i] = bp;
+          BeadArm ba;
+          if (MAT) { ba.x = lx[k]; ba.y = ly[k]; ba.z = lz[k]; }
+          else { ba.x = rx; ba.y = ry; ba.z = rz; }
+          ba.pad = 0.f;
+          barm[tbase + i] = ba;
+        }
+      }
+      // the mbarrier phase completes when lane 0 has arrived and all
+      // nuse * 128 bytes have landed (the copies may finish before the arrive)
+      if (lane == 0) mbar_arrive_expect_tx(bar, nuse * 128u);
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (use[k]) {
+          bulk_brick(bricks + (size_t)(tbase + tl + k * S) * 8, G.bricks + bidx[k] * 8, bar);
+          if (MODE == MODE_MIN) c_grid += 1;
+        }
+      }
+      // neighbour-list headers (L2-resident)
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        hdr[k] = make_uint2(0u, 0u);
+        if (nvox[k] >= 0) {
+          hdr[k] = ldg_u2(G.nb_hdr + nvox[k]);
+          if (MODE == MODE_MIN) c_look += 1;
         }
       }
 
-      acc.e = team_sum<S>(acc.e);
-      acc.gx = team_sum<S>(acc.gx);
-      acc.gy = team_sum<S>(acc.gy);
-      acc.gz = team_sum<S>(acc.gz);
+      // ---------------- phase B: flattened list offsets (team scan in bead order)
+      unsigned carry = 0;
 #pragma unroll
-      for (int k = 0; k < PoseAcc<MODE>::NT; ++k) acc.t[k] = team_sum<S>(acc.t[k]);
+      for (int k = 0; k < K; ++k) {
+        const unsigned c = hdr[k].y;
+        unsigned inc = c;
+#pragma unroll
+        for (int off = 1; off < S; off <<= 1) {
+          const unsigned t = __shfl_up_sync(0xffffffffu, inc, off, S);
+          if (tl >= off) inc += t;
+        }
+        const int i = tl + k * S;
+        if (i < N) {
+          BeadList bl;
+          bl.start = hdr[k].x;
+          bl.count = c;
+          bl.pre = carry + inc - c;
+          bl.pad = 0u;
+          blst[tbase + i] = bl;
+        }
+        carry += __shfl_sync(0xffffffffu, inc, lead + S - 1);
+      }
+      const unsigned total = carry;
+      __syncwarp();
 
-      const float etot = acc.e + p.gravity * (tx * tx + ty * ty + tz * tz);
-      if (MODE == MODE_EVAL_MAT) {
+      // ---------------- phase C: the team's flattened neighbour list
+      if (total > 0) {
+        const unsigned chunk = (total + S - 1) / S;
+        unsigned e = tl * chunk;
+        const unsigned e_end = min(total, e + chunk);
+        // bead holding entry e: the last bead whose offset is <= e
+        int bi = 0;
+        if (e < e_end) {
+          int lo = 0, hi = N - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (blst[tbase + mid].pre <= e) lo = mid; else hi = mid - 1;
+          }
+          bi = lo;
+        }
+        if (MODE == MODE_MIN) c_ent += (e < e_end) ? (e_end - e) : 0u;
+        while (e < e_end) {
+          unsigned jj[U];
+          int bb[U];
+#pragma unroll
+          for (int m = 0; m < U; ++m) {
+            jj[m] = ATT_NB_EMPTY;
+            bb[m] = bi;
+            if (e + m < e_end) {
+              BeadList bl = blst[tbase + bi];
+              while (e + m >= bl.pre + bl.count) {
+                ++bi;
+                bl = blst[tbase + bi];
+              }
+              bb[m] = bi;
+              jj[m] = ldg_u16(G.nb_list + bl.start + (e + m - bl.pre));
+            }
+          }
+#pragma unroll
+          for (int h = 0; h < U; h += 4) {
+            float4 rr[4];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+              const unsigned j = jj[h + m];
+              rr[m] = (j < (unsigned)G.n_rec) ? ldg_f4(G.rec + j) : make_float4(1e30f, 1e30f, 1e30f, 0.f);
+            }
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+              const BeadPos bp = bpos[tbase + bb[h + m]];
+              float gx, gy, gz;
+              bool hit;
+              pair_term(p, G, bp, rr[m], acc_e, gx, gy, gz, hit);
+              if (hit) {
+                const BeadArm ba = barm[tbase + bb[h + m]];
+                acc_gx += gx;
+                acc_gy += gy;
+                acc_gz += gz;
+                if (MAT) {
+                  acc_t[0] = fmaf(ba.x, gx, acc_t[0]); acc_t[1] = fmaf(ba.x, gy, acc_t[1]); acc_t[2] = fmaf(ba.x, gz, acc_t[2]);
+                  acc_t[3] = fmaf(ba.y, gx, acc_t[3]); acc_t[4] = fmaf(ba.y, gy, acc_t[4]); acc_t[5] = fmaf(ba.y, gz, acc_t[5]);
+                  acc_t[6] = fmaf(ba.z, gx, acc_t[6]); acc_t[7] = fmaf(ba.z, gy, acc_t[7]); acc_t[8] = fmaf(ba.z, gz, acc_t[8]);
+                } else {
+                  acc_t[0] = fmaf(ba.y, gz, fmaf(-ba.z, gy, acc_t[0]));
+                  acc_t[1] = fmaf(ba.z, gx, fmaf(-ba.x, gz, acc_t[1]));
+                  acc_t[2] = fmaf(ba.x, gy, fmaf(-ba.y, gx, acc_t[2]));
+                }
+              }
+            }
+          }
+          e += U;
+        }
+      }
+
+      // ---------------- phase D: grid term from the bricks in shared memory
+      {
+        bool done = false;
+        for (int it = 0; it < WAIT_LIMIT && !done; ++it) done = mbar_try_wait(bar, parity);
+        if (!__all_sync(0xffffffffu, done)) {
+          if (lane == 0) atomicOr(&g_kernel_error, ATT_KERR_COPY_TIMEOUT);
+          return;  // a bulk copy never completed: report and leave (whole warp)
+        }
+        parity ^= 1u;
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (use[k]) {
+          const float4* br = bricks + (size_t)(tbase + tl + k * S) * 8;
+          float eb = 0.f, gbx = 0.f, gby = 0.f, gbz = 0.f;
+          const float sc = gscale[k];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int c = (q + tl) & 7;  // rotated: 8 lanes hit 8 different bank groups
+            const float4 v = br[c];
+            const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
+            const float wx = cx ? fx[k] : 1.f - fx[k];
+            const float wy = cy ? fy[k] : 1.f - fy[k];
+            const float wz = cz ? fz[k] : 1.f - fz[k];
+            const float w = wx * wy * wz;
+            eb = fmaf(w, v.x, eb);
+            if (p.grad_mode == ATT_GRAD_REFERENCE) {
+              gbx = fmaf(-w, v.y, gbx);
+              gby = fmaf(-w, v.z, gby);
+              gbz = fmaf(-w, v.w, gbz);
+            } else {
+              const float ce = v.x * sc;
+              gbx = fmaf(ce, (cx ? 1.f : -1.f) * wy * wz, gbx);
+              gby = fmaf(ce, wx * (cy ? 1.f : -1.f) * wz, gby);
+              gbz = fmaf(ce, wx * wy * (cz ? 1.f : -1.f), gbz);
+            }
+            if (MODE == MODE_BWD) {
+              float* dg = outer_k[k] ? p.dgrid_outer : p.dgrid_inner;
+              if (dg != nullptr) {
+                const int nx = outer_k[k] ? G.dx2 : G.dx;
+                const int ny = outer_k[k] ? G.dy2 : G.dy;
+                const int nz = outer_k[k] ? G.dz2 : G.dz;
+                const long long off =
+                    ((((long long)brick_gt[k] * nx + bix[k] + cx) * ny + biy[k] + cy) * (long long)nz + biz[k] + cz) * 4;
+                atomicAdd(dg + off, dLdE * w);
+              }
+            }
+          }
+          const BeadArm ba = barm[tbase + tl + k * S];
+          acc_e += eb;
+          acc_gx += gbx;
+          acc_gy += gby;
+          acc_gz += gbz;
+          if (MAT) {
+            acc_t[0] = fmaf(ba.x, gbx, acc_t[0]); acc_t[1] = fmaf(ba.x, gby, acc_t[1]); acc_t[2] = fmaf(ba.x, gbz, acc_t[2]);
+            acc_t[3] = fmaf(ba.y, gbx, acc_t[3]); acc_t[4] = fmaf(ba.y, gby, acc_t[4]); acc_t[5] = fmaf(ba.y, gbz, acc_t[5]);
+            acc_t[6] = fmaf(ba.z, gbx, acc_t[6]); acc_t[7] = fmaf(ba.z, gby, acc_t[7]); acc_t[8] = fmaf(ba.z, gbz, acc_t[8]);
+          } else {
+            acc_t[0] = fmaf(ba.y, gbz, fmaf(-ba.z, gby, acc_t[0]));
+            acc_t[1] = fmaf(ba.z, gbx, fmaf(-ba.x, gbz, acc_t[1]));
+            acc_t[2] = fmaf(ba.x, gby, fmaf(-ba.y, gbx, acc_t[2]));
+          }
+        }
+      }
+      // the next chunk's / evaluation's bulk copies overwrite the slots read above
+      __syncwarp();
+      fence_proxy_async();
+      }  // chunks
+
+      // ---------------- team reduction and output / ADAM
+      acc_e = team_sum<S>(acc_e);
+      acc_gx = team_sum<S>(acc_gx);
+      acc_gy = team_sum<S>(acc_gy);
+      acc_gz = team_sum<S>(acc_gz);
+#pragma unroll
+      for (int k = 0; k < (MAT ? 9 : 3); ++k) acc_t[k] = team_sum<S>(acc_t[k]);
+
+      const float etot = acc_e + p.gravity * (tx * tx + ty * ty + tz * tz);
+      if (MAT) {
         if (valid) {
           if (tl == 0) p.energy[b] = etot;
           if (p.grad != nullptr) {
@@ -297,22 +558,23 @@ __global__ void __launch_bounds__(256) score_kernel(const __grid_constant__ KPar
               const int r = k >> 2, c = k & 3;
               float v = 0.f;
               if (c < 3) {
-                if (r < 3) v = acc.t[r * 3 + c];
-                else v = (c == 0) ? acc.gx : (c == 1 ? acc.gy : acc.gz);
+                if (r < 3) v = acc_t[r * 3 + c];
+                else v = (c == 0) ? acc_gx : (c == 1 ? acc_gy : acc_gz);
               }
               p.grad[(long long)b * 16 + k] = v;
             }
           }
+          if (tl == 0 && p.status != nullptr) p.status[b] = isfinite(etot) ? 0 : ATT_STATUS_NONFINITE_ENERGY;
         }
         break;
       }
       // pose gradient: dE/dt and dE/d(angle_k) = w_k . torque
-      const float gtx = acc.gx + 2.f * p.gravity * tx;
-      const float gty = acc.gy + 2.f * p.gravity * ty;
-      const float gtz = acc.gz + 2.f * p.gravity * tz;
-      const float gphi = acc.t[2];
-      const float gpsi = -sphi * acc.t[0] + cphi * acc.t[1];
-      const float gth = -(cphi * spsi * acc.t[0] + sphi * spsi * acc.t[1] + cpsi * acc.t[2]);
+      const float gtx = acc_gx + 2.f * p.gravity * tx;
+      const float gty = acc_gy + 2.f * p.gravity * ty;
+      const float gtz = acc_gz + 2.f * p.gravity * tz;
+      const float gphi = acc_t[2];
+      const float gpsi = -sphi * acc_t[0] + cphi * acc_t[1];
+      const float gth = -(cphi * spsi * acc_t[0] + sphi * spsi * acc_t[1] + cpsi * acc_t[2]);
       float gk = gphi;
       gk = (tl == 1) ? gpsi : gk;
       gk = (tl == 2) ? gth : gk;
@@ -332,7 +594,7 @@ __global__ void __launch_bounds__(256) score_kernel(const __grid_constant__ KPar
         }
         break;
       }
-      // ---- fused ADAM step on lanes 0..5 (optax.adam form) ----
+      // ---- fused ADAM step on lanes 0..5 (optax.adam form)
       const bool ok = isfinite(gtx) & isfinite(gty) & isfinite(gtz) & isfinite(gphi) & isfinite(gpsi) &
                       isfinite(gth);
       if (!ok) {
@@ -348,13 +610,11 @@ __global__ void __launch_bounds__(256) score_kernel(const __grid_constant__ KPar
       }
     }
 
-    if (MODE == MODE_MIN && valid) {
-      if (tl < 6) {
-        p.pose_out[(long long)b * 6 + tl] = my_x;
-        if (p.adam != nullptr) {
-          p.adam[(long long)b * 12 + tl] = my_m;
-          p.adam[(long long)b * 12 + 6 + tl] = my_v;
-        }
+    if (MODE == MODE_MIN && valid && tl < 6) {
+      p.pose_out[(long long)b * 6 + tl] = my_x;
+      if (p.adam != nullptr) {
+        p.adam[(long long)b * 12 + tl] = my_m;
+        p.adam[(long long)b * 12 + 6 + tl] = my_v;
       }
     }
     if ((MODE == MODE_MIN || MODE == MODE_EVAL) && valid && tl == 0 && p.status != nullptr) p.status[b] = status;
@@ -380,49 +640,78 @@ __global__ void __launch_bounds__(256) score_kernel(const __grid_constant__ KPar
 }
 
 // ---------------------------------------------------------------------------
-// launchers
+// launch plumbing: (S, K) instantiations and their shared-memory needs
 // ---------------------------------------------------------------------------
 template <int MODE>
-static cudaError_t launch_mode(const KParams& p, int S, int blocks, int threads, cudaStream_t st) {
-  switch (S) {
-    case 8: score_kernel<8, MODE><<<blocks, threads, 0, st>>>(p); break;
-    case 16: score_kernel<16, MODE><<<blocks, threads, 0, st>>>(p); break;
-    case 32: score_kernel<32, MODE><<<blocks, threads, 0, st>>>(p); break;
-    default: return cudaErrorInvalidValue;
+struct KernelTable {
+  static const void* get(int S, int K) {
+#define ATT_CASE(s_, k_) \
+  if (S == s_ && K == k_) return (const void*)score_kernel<s_, k_, MODE>;
+    ATT_CASE(32, 1) ATT_CASE(32, 2) ATT_CASE(32, 4) ATT_CASE(32, 8)
+    ATT_CASE(16, 1) ATT_CASE(16, 2) ATT_CASE(16, 4) ATT_CASE(16, 8)
+    ATT_CASE(8, 1) ATT_CASE(8, 2) ATT_CASE(8, 4) ATT_CASE(8, 8)
+#undef ATT_CASE
+    return nullptr;
   }
-  return cudaGetLastError();
+};
+
+static size_t smem_per_warp(int K) {
+  switch (K) {
+    case 1: return warp_smem_bytes<1>();
+    case 2: return warp_smem_bytes<2>();
+    case 4: return warp_smem_bytes<4>();
+    case 8: return warp_smem_bytes<8>();
+  }
+  return 0;
 }
 
-template <int MODE>
-static const void* kernel_ptr(int S) {
-  switch (S) {
-    case 8: return (const void*)score_kernel<8, MODE>;
-    case 16: return (const void*)score_kernel<16, MODE>;
-    case 32: return (const void*)score_kernel<32, MODE>;
+static const void* kernel_of(int mode, int S, int K) {
+  switch (mode) {
+    case MODE_EVAL: return KernelTable<MODE_EVAL>::get(S, K);
+    case MODE_EVAL_MAT: return KernelTable<MODE_EVAL_MAT>::get(S, K);
+    case MODE_MIN: return KernelTable<MODE_MIN>::get(S, K);
+    case MODE_BWD: return KernelTable<MODE_BWD>::get(S, K);
   }
   return nullptr;
 }
 
-cudaError_t launch_score(const KParams& p, int mode, int S, int blocks, int threads, cudaStream_t st) {
-  switch (mode) {
-    case MODE_EVAL: return launch_mode<MODE_EVAL>(p, S, blocks, threads, st);
-    case MODE_EVAL_MAT: return launch_mode<MODE_EVAL_MAT>(p, S, blocks, threads, st);
-    case MODE_MIN: return launch_mode<MODE_MIN>(p, S, blocks, threads, st);
-    case MODE_BWD: return launch_mode<MODE_BWD>(p, S, blocks, threads, st);
-  }
-  return cudaErrorInvalidValue;
+int beads_per_lane(int S, int max_beads) {
+  const int need = (max_beads + S - 1) / S;
+  int K = 1;
+  while (K < need) K <<= 1;
+  return K <= ATT_MAX_BEADS_PER_LANE ? K : ATT_MAX_BEADS_PER_LANE;  // larger ligands run in chunks
 }
 
-cudaError_t occupancy_blocks(int mode, int S, int threads, int* blocks_per_sm) {
-  const void* k = nullptr;
-  switch (mode) {
-    case MODE_EVAL: k = kernel_ptr<MODE_EVAL>(S); break;
-    case MODE_EVAL_MAT: k = kernel_ptr<MODE_EVAL_MAT>(S); break;
-    case MODE_MIN: k = kernel_ptr<MODE_MIN>(S); break;
-    case MODE_BWD: k = kernel_ptr<MODE_BWD>(S); break;
-  }
+size_t score_smem_bytes(int K, int threads) { return smem_per_warp(K) * (size_t)(threads / 32); }
+
+cudaError_t launch_score(const KParams& p, int mode, int S, int K, int blocks, int threads, cudaStream_t st) {
+  const void* k = kernel_of(mode, S, K);
   if (k == nullptr) return cudaErrorInvalidValue;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k, threads, 0);
+  const size_t smem = score_smem_bytes(K, threads);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  void* args[] = {const_cast<KParams*>(&p)};
+  return cudaLaunchKernel(k, dim3(blocks), dim3(threads), args, smem, st);
+}
+
+cudaError_t kernel_status(int* out, int clear, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyFromSymbolAsync(out, g_kernel_error, sizeof(int), 0, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && clear && *out) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbolAsync(g_kernel_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  return e;
+}
+
+cudaError_t occupancy_blocks(int mode, int S, int K, int threads, int* blocks_per_sm) {
+  const void* k = kernel_of(mode, S, K);
+  if (k == nullptr) return cudaErrorInvalidValue;
+  const size_t smem = score_smem_bytes(K, threads);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k, threads, smem);
 }
 
 }  // namespace att

@@ -52,6 +52,14 @@ extern "C" {
 #define ATT_STATUS_NONFINITE_GRAD 1   /* a step saw a non-finite gradient and was skipped */
 #define ATT_STATUS_NONFINITE_ENERGY 2 /* the returned energy is not finite */
 
+/* device-wide kernel error word (att_kernel_status) */
+#define ATT_KERR_COPY_TIMEOUT 1 /* a warp gave up waiting for its grid-brick bulk copies and returned */
+
+/* A pose is served by lanes_per_pose lanes holding up to 8 beads each; a
+   ligand with more than 8 * lanes_per_pose beads is evaluated in chunks of that
+   many beads (slower: its coordinates are re-read every chunk). */
+#define ATT_MAX_BEADS_PER_LANE 8
+
 /* Geometry of one receptor grid: the scalar fields of read_grid2.py's Grid. */
 typedef struct AttGridGeom {
   float origin[3];  /* position of inner grid point (0,0,0) */
@@ -116,7 +124,7 @@ typedef struct AttAdamCfg {
 /* Launch shape; zeros pick the defaults / autotuned values. */
 typedef struct AttLaunchCfg {
   int lanes_per_pose;   /* 8, 16 or 32 (poses per warp = 32 / lanes_per_pose) */
-  int block_threads;    /* multiple of 32, <= 1024 */
+  int block_threads;    /* 32, 64, 96 or 128 (0 = 128) */
   int blocks;           /* persistent CTAs (att_minimise), 0 = fill the GPU */
   int pad_;
 } AttLaunchCfg;
@@ -188,6 +196,12 @@ int att_nbgrid_count(const AttGridGeom* geom, const float* rec_dev, int n_rec, f
                      long long workspace_bytes, void* stream);
 int att_nbgrid_fill(const AttGridGeom* geom, const float* rec_dev, int n_rec, float radius,
                     const uint32_t* hdr_dev, uint16_t* list_dev, void* stream);
+
+/* Read the device-wide error word of the scoring kernels (ATT_KERR_* bits, 0 =
+   none) into *error_word, clearing it if `clear`; synchronises `stream`.  A
+   non-zero word means some warp stopped early and its poses' outputs are stale.
+   (No counterpart in the reference: JAX has no device-side waits.) */
+int att_kernel_status(int* error_word, int clear, void* stream);
 
 #ifdef __cplusplus
 }

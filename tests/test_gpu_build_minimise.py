@@ -181,3 +181,41 @@ def test_minimise_stats_counts():
     assert 0 < st[0] <= 4 * 32 * n_lig
     assert 0 < st[1] <= 4 * 32 * n_lig
     assert st[2] >= 0
+
+
+def test_large_ligands_and_chunking():
+    """Ligands up to 8 beads per lane (256 at 32 lanes per pose) and larger
+    ones, evaluated in chunks, match the oracle; teams of one warp with
+    different chunk counts (conformers of mixed size are not allowed, so mixed
+    segments) also do."""
+    A = _A()
+    c = small_case(seed=19, n_poses=16)
+    grid = to_device_grid(c)
+    rng = np.random.default_rng(5)
+    for n, lanes in ((200, 32), (64, 8), (33, 16), (65, 8), (300, 32), (150, 16)):
+        lig = (rng.normal(size=(n, 3)) * 2.0).astype(np.float32).astype(np.float64)
+        gt = rng.integers(0, 4, n)
+        wl = A.Workload([grid], A.LigandSet([(lig, gt, gt)]), [A.Segment(0, 0, 16)], lanes_per_pose=lanes)
+        P = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+        E, G, _ = A.energrad(wl, P)
+        Eo, Go = O.energrad(c["poses"], lig, gt, gt, c["G"])
+        assert np.allclose(E.cpu().numpy(), Eo, rtol=2e-5, atol=2e-3), (n, lanes)
+    # one warp, teams with 1 and 3 chunks (8 lanes x 8 beads = 64 per chunk)
+    ligs = [((rng.normal(size=(n, 3)) * 2.0).astype(np.float32).astype(np.float64), rng.integers(0, 4, n))
+            for n in (20, 150)]
+    wl = A.Workload([grid], A.LigandSet([(x, t, t) for x, t in ligs]), [A.Segment(0, 0, 3), A.Segment(0, 1, 5)],
+                    lanes_per_pose=8)
+    P = torch.tensor(c["poses"][:8], dtype=torch.float32, device="cuda")
+    E, _, _ = A.minimise(wl, P, 2)[1], None, None
+    for seg, (x, t), sl in ((0, ligs[0], slice(0, 3)), (1, ligs[1], slice(3, 8))):
+        w1 = A.Workload([grid], A.LigandSet([(x, t, t)]), [A.Segment(0, 0, sl.stop - sl.start)], lanes_per_pose=8)
+        E1 = A.minimise(w1, P[sl].contiguous(), 2)[1]
+        assert torch.equal(E1, E[sl])
+
+
+def test_zz_kernel_error_word_is_clear():
+    """No warp of any kernel above gave up on a bulk copy."""
+    from attract_b200 import _lib
+
+    torch.cuda.synchronize()
+    assert _lib.kernel_status(clear=True) == 0

@@ -81,6 +81,7 @@ SIGNATURES = {
     "att_nbgrid_count": (I, [C.POINTER(AttGridGeom), P, I, F, P, P, P, LL, P]),
     "att_nbgrid_fill": (I, [C.POINTER(AttGridGeom), P, I, F, P, P, P]),
     "att_kernel_status": (I, [C.POINTER(C.c_int), I, P]),
+    "att_nbgrid_count_noalloc": (I, [C.POINTER(AttGridGeom), P, I, F, P, P, P]),
 }
 
 _lib = None

@@ -283,3 +283,86 @@ cudaError_t launch_repack(const AttGridGeom& g, const float* inner, const float*
 }
 
 }  // namespace att
+
+// ---------------------------------------------------------------------------
+// att_nbgrid_count_noalloc: the neighbour-list count + scan of
+// att_nbgrid_count with its scan workspace (one word per 1024 grid points) in
+// a fixed device array of this library instead of caller memory, for callers
+// that cannot allocate device memory themselves.
+// ---------------------------------------------------------------------------
+#include <mutex>
+#include <stdio.h>
+
+namespace att {
+int report_error(int code, const char* msg);
+}
+
+// Fixed scan workspace: 8192 words = 32 KB, i.e. grids of up to 8192 * 1024
+// inner points.  Every device that loads the library holds it until exit.
+static __device__ __align__(256) unsigned g_nbgrid_scan_ws[ATT_NBGRID_NOALLOC_MAX_VOXELS / 1024];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scan_ws_mutex;
+void* g_scan_ws_addr[kMaxDevices] = {};  // device address of g_nbgrid_scan_ws, per device
+
+// Device address of the fixed workspace on the current device.  The name
+// g_nbgrid_scan_ws in host code is only a host-side stand-in for the symbol;
+// the kernel must be given the address that cudaGetSymbolAddress returns for
+// the device that is current.  Looked up once per device, on the first call.
+int scan_ws_address(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return att::report_error(ATT_E_CUDA, "att_nbgrid_count_noalloc: cudaGetDevice failed");
+  if (dev < 0 || dev >= kMaxDevices)
+    return att::report_error(ATT_E_UNSUPPORTED, "att_nbgrid_count_noalloc: device index beyond 64");
+  std::lock_guard<std::mutex> lock(g_scan_ws_mutex);
+  if (g_scan_ws_addr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_nbgrid_scan_ws);
+    if (e != cudaSuccess || p == nullptr) {
+      char msg[256];
+      snprintf(msg, sizeof(msg), "att_nbgrid_count_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
+               cudaGetErrorString(e));
+      return att::report_error(ATT_E_CUDA, msg);
+    }
+    g_scan_ws_addr[dev] = p;
+  }
+  *out = g_scan_ws_addr[dev];
+  return ATT_OK;
+}
+}  // namespace
+
+extern "C" int att_nbgrid_count_noalloc(const AttGridGeom* geom, const float* rec_dev, int n_rec, float radius,
+                                        uint32_t* hdr_dev, unsigned long long* total_dev, void* stream) {
+  char msg[256];
+  if (geom == nullptr) return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: geometry is NULL");
+  for (int k = 0; k < 3; ++k) {
+    if (geom->dim[k] < 2) return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: dim must be >= 2");
+  }
+  if (!(geom->spacing > 0.f)) return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: spacing must be > 0");
+  const long long nvox = (long long)geom->dim[0] * geom->dim[1] * geom->dim[2];
+  if (nvox > ATT_NBGRID_NOALLOC_MAX_VOXELS) {
+    snprintf(msg, sizeof(msg),
+             "att_nbgrid_count_noalloc: %lld grid points exceed the fixed workspace (at most %lld); "
+             "use att_nbgrid_count with a caller-provided workspace",
+             nvox, (long long)ATT_NBGRID_NOALLOC_MAX_VOXELS);
+    return att::report_error(ATT_E_INVALID, msg);
+  }
+  if (n_rec < 0 || n_rec >= (int)ATT_NB_EMPTY || (n_rec > 0 && rec_dev == nullptr))
+    return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: receptor beads");
+  if (hdr_dev == nullptr || total_dev == nullptr)
+    return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: NULL output");
+  if (!(radius >= 0.f)) return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: radius < 0");
+  void* ws = nullptr;
+  int rc = scan_ws_address(&ws);
+  if (rc != ATT_OK) return rc;
+  // every workspace word the scan reads is written by the count kernel of the
+  // same call first, so nothing has to be cleared between calls
+  cudaError_t e = att::launch_nb_count(*geom, rec_dev, n_rec, radius, hdr_dev, total_dev, ws, (cudaStream_t)stream);
+  if (e != cudaSuccess) {
+    snprintf(msg, sizeof(msg), "att_nbgrid_count_noalloc: %s", cudaGetErrorString(e));
+    return att::report_error(ATT_E_CUDA, msg);
+  }
+  return ATT_OK;
+}

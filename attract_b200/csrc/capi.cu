@@ -35,6 +35,11 @@ static int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+namespace att {
+// error reporting for entry points defined in other translation units
+int report_error(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace att
+
 static int cuda_fail(cudaError_t e, const char* where) {
   return fail(ATT_E_CUDA, "%s: %s (%s)", where, cudaGetErrorString(e), cudaGetErrorName(e));
 }

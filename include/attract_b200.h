@@ -197,6 +197,25 @@ int att_nbgrid_count(const AttGridGeom* geom, const float* rec_dev, int n_rec, f
 int att_nbgrid_fill(const AttGridGeom* geom, const float* rec_dev, int n_rec, float radius,
                     const uint32_t* hdr_dev, uint16_t* list_dev, void* stream);
 
+/* att_nbgrid_count without a caller workspace.  No counterpart in the
+   reference (its neighbour lists come from a KD-tree on the host).
+   Some callers of this library cannot allocate device memory: a plugin that
+   only receives the buffers of a host framework owning all GPU memory through
+   its own allocator, a C/FFI binding with no allocator of its own, or a
+   latency-bound service that must never call cudaMalloc/cudaFree (they
+   synchronise the device).  This entry point takes the same inputs and
+   outputs as att_nbgrid_count but keeps the scan workspace in a fixed array
+   inside the library (32 KB on every device that loads it, held until exit),
+   so it allocates nothing: grids of at most ATT_NBGRID_NOALLOC_MAX_VOXELS inner
+   points; larger grids are rejected with ATT_E_INVALID.  The first call on a
+   device looks up the array's device address (cudaGetSymbolAddress) with that
+   device current; make that first call before any stream capture.  All calls
+   share the one array: calls that overlap on the GPU (other streams, other
+   host threads) race on it and must be serialised by the caller. */
+#define ATT_NBGRID_NOALLOC_MAX_VOXELS (8192LL * 1024LL)
+int att_nbgrid_count_noalloc(const AttGridGeom* geom, const float* rec_dev, int n_rec, float radius,
+                             uint32_t* hdr_dev, unsigned long long* total_dev, void* stream);
+
 /* Read the device-wide error word of the scoring kernels (ATT_KERR_* bits, 0 =
    none) into *error_word, clearing it if `clear`; synchronises `stream`.  A
    non-zero word means some warp stopped early and its poses' outputs are stale.

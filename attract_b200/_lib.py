@@ -35,7 +35,8 @@ class AttGrid(C.Structure):
     _fields_ = [("geom", AttGridGeom), ("bricks", C.c_void_p), ("n_inner_bricks", C.c_longlong),
                 ("n_outer_bricks", C.c_longlong), ("nb_hdr", C.c_void_p), ("nb_list", C.c_void_p),
                 ("n_nb_entries", C.c_longlong), ("rec", C.c_void_p), ("n_rec", C.c_int),
-                ("n_rtypes", C.c_int), ("n_ltypes", C.c_int), ("pad_", C.c_int), ("pair", C.c_void_p)]
+                ("n_rtypes", C.c_int), ("n_ltypes", C.c_int), ("nb_rec_bytes", C.c_int), ("pair", C.c_void_p),
+                ("nb_rec", C.c_void_p)]
 
 
 class AttLigands(C.Structure):
@@ -82,16 +83,21 @@ SIGNATURES = {
     "att_nbgrid_fill": (I, [C.POINTER(AttGridGeom), P, I, F, P, P, P]),
     "att_kernel_status": (I, [C.POINTER(C.c_int), I, P]),
     "att_nbgrid_count_noalloc": (I, [C.POINTER(AttGridGeom), P, I, F, P, P, P]),
+    "att_nbgrid_pack_records": (I, [P, P, LL, I, P, P]),
+    "att_kernel_debug_info": (I, [C.POINTER(C.c_ulonglong), I, P]),
 }
 
 _lib = None
 
 
-def load(path: str = LIB_PATH):
-    """Load the library once; raises if it has not been built."""
+def load(path: str | None = None):
+    """Load the library once; raises if it has not been built.  The path may be
+    overridden with $ATTRACT_B200_LIB (another build of the same sources)."""
     global _lib
     if _lib is not None:
         return _lib
+    if path is None:
+        path = os.environ.get("ATTRACT_B200_LIB", LIB_PATH)
     if not os.path.exists(path):
         raise AttractError(
             f"{path} is missing: build it with `python -m attract_b200.build` (nvcc, sm_100a); "

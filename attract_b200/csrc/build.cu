@@ -246,6 +246,28 @@ cudaError_t launch_nb_fill(const AttGridGeom& g, const float* rec, int n_rec, fl
   return cudaGetLastError();
 }
 
+// CSR -> fixed-size records {u32 overflow index, u16 count, inline entries}
+__global__ void nb_pack_kernel(const uint2* __restrict__ hdr, const uint16_t* __restrict__ list, long long nvox,
+                               int rec_bytes, unsigned char* __restrict__ out) {
+  const int inl = ATT_NB_INLINE(rec_bytes);
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
+       v += (long long)gridDim.x * blockDim.x) {
+    const uint2 h = hdr[v];
+    unsigned char* r = out + v * rec_bytes;
+    *reinterpret_cast<unsigned*>(r) = h.x + (unsigned)inl;
+    uint16_t* e = reinterpret_cast<uint16_t*>(r + 4);
+    e[0] = (uint16_t)min(h.y, 65535u);
+    for (int i = 0; i < inl; ++i) e[1 + i] = (i < (int)h.y) ? list[h.x + i] : (uint16_t)ATT_NB_EMPTY;
+  }
+}
+
+cudaError_t launch_nb_pack(const uint32_t* hdr, const uint16_t* list, long long nvox, int rec_bytes, void* out,
+                           cudaStream_t st) {
+  nb_pack_kernel<<<148 * 8, 256, 0, st>>>(reinterpret_cast<const uint2*>(hdr), list, nvox, rec_bytes,
+                                          reinterpret_cast<unsigned char*>(out));
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // K5: dense [T][X][Y][Z][4] -> bricks [T][inner+outer][8 corners]
 // ---------------------------------------------------------------------------

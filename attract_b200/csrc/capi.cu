@@ -7,10 +7,11 @@
 
 namespace att {
 cudaError_t launch_score(const KParams& p, int mode, int S, int K, int blocks, int threads, cudaStream_t st);
-cudaError_t occupancy_blocks(int mode, int S, int K, int threads, int* blocks_per_sm);
+cudaError_t occupancy_blocks(int mode, int S, int K, int threads, int rec_slot, int* blocks_per_sm);
 cudaError_t kernel_status(int* out, int clear, cudaStream_t st);
+cudaError_t kernel_debug_info(unsigned long long* out3, int clear, cudaStream_t st);
 int beads_per_lane(int S, int max_beads);
-size_t score_smem_bytes(int K, int threads);
+size_t score_smem_bytes(int K, int threads, int rec_slot);
 cudaError_t launch_build_potential(const AttGridGeom& g, const float* rec, int n_rec, const float* pair,
                                    int n_rtypes, int n_ltypes, float cutoff, int outer, float* out,
                                    cudaStream_t st);
@@ -21,6 +22,8 @@ cudaError_t launch_nb_fill(const AttGridGeom& g, const float* rec, int n_rec, fl
                            uint16_t* list, cudaStream_t st);
 cudaError_t launch_repack(const AttGridGeom& g, const float* inner, const float* outer, void* bricks,
                           cudaStream_t st);
+cudaError_t launch_nb_pack(const uint32_t* hdr, const uint16_t* list, long long nvox, int rec_bytes, void* out,
+                           cudaStream_t st);
 }  // namespace att
 
 using namespace att;
@@ -53,6 +56,10 @@ extern "C" const char* att_last_error_string(void) { return g_err; }
 extern "C" const char* att_version(void) { return "attract_b200 0.1 (sm_100a)"; }
 
 static bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+// dynamic shared memory per block of the scoring kernels: 227 KB less the
+// static grid-descriptor copies (ATT_MAX_GRIDS KGrid) and slack
+static const size_t kDynSmemLimit = 227 * 1024 - 4096;
 
 static int check_geom(const AttGridGeom* g) {
   REQUIRE(g != nullptr, "geometry is NULL");
@@ -98,6 +105,9 @@ static int make_kgrid(const AttGrid* a, int gi, KGrid* k) {
   if (a->nb_hdr != nullptr) {
     REQUIRE(aligned(a->nb_hdr, 8), "grid %d: nb_hdr not 8-B aligned", gi);
     REQUIRE(a->n_nb_entries == 0 || a->nb_list != nullptr, "grid %d: nb_list is NULL", gi);
+    REQUIRE(a->nb_rec != nullptr && aligned(a->nb_rec, 16), "grid %d: nb_rec NULL or not 16-B aligned", gi);
+    REQUIRE(a->nb_rec_bytes == 32 || a->nb_rec_bytes == 64 || a->nb_rec_bytes == 128,
+            "grid %d: nb_rec_bytes = %d (32, 64 or 128)", gi, a->nb_rec_bytes);
   }
   memset(k, 0, sizeof(*k));
   k->ox = g.origin[0];
@@ -126,9 +136,17 @@ static int make_kgrid(const AttGrid* a, int gi, KGrid* k) {
   k->has_outer = (a->bricks != nullptr && a->n_outer_bricks > 0) ? 1 : 0;
   k->type_stride = ni + (k->has_outer ? a->n_outer_bricks : 0);
   k->n_inner = ni;
+  k->n_list = a->n_nb_entries;
+  k->n_vox = (long long)g.dim[0] * g.dim[1] * g.dim[2];
+  k->n_bricks = (long long)g.n_types * k->type_stride;
   k->bricks = reinterpret_cast<const float4*>(a->bricks);
   k->nb_hdr = reinterpret_cast<const uint2*>(a->nb_hdr);
   k->nb_list = a->nb_list;
+  if (a->nb_hdr != nullptr) {
+    k->nb_rec = reinterpret_cast<const unsigned char*>(a->nb_rec);
+    k->nb_rec_bytes = a->nb_rec_bytes;
+    k->nb_inline = ATT_NB_INLINE(a->nb_rec_bytes);
+  }
   k->rec = reinterpret_cast<const float4*>(a->rec);
   k->pair = reinterpret_cast<const float4*>(a->pair);
   return ATT_OK;
@@ -154,16 +172,23 @@ static int fill_common(KParams* p, const AttGrid* grids, int n_grids, const AttL
   *S = s;
   REQUIRE(ligs->max_beads >= 1, "ligands: max_beads = %d", ligs->max_beads);
   *K = beads_per_lane(s, ligs->max_beads);
-  const int t = (launch && launch->block_threads) ? launch->block_threads : 128;
+  int t = (launch && launch->block_threads) ? launch->block_threads : 128;
   REQUIRE(t == 32 || t == 64 || t == 96 || t == 128, "block_threads = %d (32, 64, 96 or 128)", t);
-  REQUIRE(score_smem_bytes(*K, t) <= 227 * 1024, "%d threads x %d beads per lane need %zu B of shared memory", t,
-          *K, score_smem_bytes(*K, t));
   *threads = t;
   memset(p, 0, sizeof(*p));
+  int rec_slot = 0;  // neighbour-record slot: the largest record of any grid
   for (int i = 0; i < n_grids; ++i) {
     int rc = make_kgrid(&grids[i], i, &p->grid[i]);
     if (rc) return rc;
+    if (p->grid[i].nb_rec_bytes > rec_slot) rec_slot = p->grid[i].nb_rec_bytes;
   }
+  p->rec_slot = rec_slot;
+  if (!(launch && launch->block_threads)) {  // default: the largest block whose shared memory fits
+    while (t > 32 && score_smem_bytes(*K, t, rec_slot) > kDynSmemLimit) t -= 32;
+    *threads = t;
+  }
+  REQUIRE(score_smem_bytes(*K, t, rec_slot) <= kDynSmemLimit,
+          "%d threads x %d beads per lane need %zu B of shared memory", t, *K, score_smem_bytes(*K, t, rec_slot));
   p->lig_beads = reinterpret_cast<const float4*>(ligs->beads);
   p->lig_off = ligs->offset;
   p->segs = segs;
@@ -201,7 +226,8 @@ extern "C" int att_energrad(const AttGrid* grids, int n_grids, const AttLigands*
   return ATT_OK;
 }
 
-static int persistent_blocks(int mode, int S, int K, int threads, const AttLaunchCfg* launch, int n_tiles, int* blocks) {
+static int persistent_blocks(int mode, int S, int K, int threads, int rec_slot, const AttLaunchCfg* launch, int n_tiles,
+                             int* blocks) {
   if (launch && launch->blocks > 0) {
     *blocks = launch->blocks;
     return ATT_OK;
@@ -209,7 +235,7 @@ static int persistent_blocks(int mode, int S, int K, int threads, const AttLaunc
   int dev = 0, sms = 0, per = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess) e = occupancy_blocks(mode, S, K, threads, &per);
+  if (e == cudaSuccess) e = occupancy_blocks(mode, S, K, threads, rec_slot, &per);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   if (per < 1) per = 1;
   const int wpb = threads / 32;
@@ -256,7 +282,7 @@ extern "C" int att_minimise(const AttGrid* grids, int n_grids, const AttLigands*
   p.step0 = cfg->step0;
   if (n_tiles == 0) return ATT_OK;
   int blocks = 0;
-  rc = persistent_blocks(MODE_MIN, S, K, threads, launch, n_tiles, &blocks);
+  rc = persistent_blocks(MODE_MIN, S, K, threads, p.rec_slot, launch, n_tiles, &blocks);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e = cudaMemsetAsync(work_counter_dev, 0, sizeof(int), st);
@@ -282,6 +308,11 @@ extern "C" int att_energrad_backward(const AttGrid* grids, int n_grids, const At
   p.dLdpose = dL_dpose_dev;
   p.dgrid_inner = dgrid_inner_dev;
   p.dgrid_outer = dgrid_outer_dev;
+  {
+    const AttGridGeom& g = grids[0].geom;
+    p.n_dgrid_inner = (long long)g.n_types * g.dim[0] * g.dim[1] * g.dim[2] * 4;
+    p.n_dgrid_outer = (long long)g.n_types * g.dim2[0] * g.dim2[1] * g.dim2[2] * 4;
+  }
   if (n_tiles == 0) return ATT_OK;
   const int wpb = threads / 32;
   const int blocks = (n_tiles + wpb - 1) / wpb;
@@ -319,6 +350,25 @@ extern "C" int att_build_potential_grid(const AttGridGeom* geom, const float* re
   cudaError_t e = launch_build_potential(*geom, rec_dev, n_rec, pair_dev, n_rtypes, n_ltypes, cutoff, outer,
                                          out_dev, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(e, "att_build_potential_grid");
+  return ATT_OK;
+}
+
+extern "C" int att_nbgrid_pack_records(const uint32_t* hdr_dev, const uint16_t* list_dev, long long n_voxels,
+                                       int rec_bytes, void* records_dev, void* stream) {
+  REQUIRE(rec_bytes == 32 || rec_bytes == 64 || rec_bytes == 128, "rec_bytes = %d (32, 64 or 128)", rec_bytes);
+  REQUIRE(n_voxels >= 0, "n_voxels < 0");
+  REQUIRE(hdr_dev != nullptr && list_dev != nullptr && records_dev != nullptr, "hdr / list / records NULL");
+  REQUIRE(aligned(hdr_dev, 8) && aligned(records_dev, 16), "hdr 8-B / records 16-B alignment");
+  if (n_voxels == 0) return ATT_OK;
+  cudaError_t e = launch_nb_pack(hdr_dev, list_dev, n_voxels, rec_bytes, records_dev, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "att_nbgrid_pack_records");
+  return ATT_OK;
+}
+
+extern "C" int att_kernel_debug_info(unsigned long long* info3, int clear, void* stream) {
+  REQUIRE(info3 != nullptr, "info3 is NULL");
+  cudaError_t e = kernel_debug_info(info3, clear, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "att_kernel_debug_info");
   return ATT_OK;
 }
 

@@ -24,7 +24,13 @@ struct __align__(16) KGrid {
   long long n_inner;              // inner bricks per type
   const float4* bricks;           // NULL: no potential grid
   const uint2* nb_hdr;            // NULL: no neighbour grid
-  const uint16_t* nb_list;
+  const uint16_t* nb_list;        // CSR entries (the records' overflow)
+  const unsigned char* nb_rec;    // fixed-size records, one per inner grid point
+  int nb_rec_bytes;               // record size
+  int nb_inline;                  // entries held inline in a record
+  long long n_list;               // CSR entries, records (= inner grid points), bricks (all types):
+  long long n_vox;                //   sizes for the bounds checks of ATT_BOUNDS_CHECK builds
+  long long n_bricks;
   const float4* rec;
   const float4* pair;             // [n_ltypes][n_rtypes][2] float4
 };
@@ -57,6 +63,9 @@ struct KParams {
   float gravity;
   float lr_rot, lr_trans, b1, b2, eps;
   int step0;
+  int rec_slot;          // bytes of a neighbour-record slot in shared memory (max over grids)
+  long long n_lig_beads;   // sizes for ATT_BOUNDS_CHECK builds
+  long long n_dgrid_inner, n_dgrid_outer;
 };
 
 __device__ __forceinline__ float4 ldg_f4(const float4* p) { return __ldg(p); }

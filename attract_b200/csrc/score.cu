@@ -72,14 +72,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // 128-byte brick: global -> shared through the bulk-copy (TMA) engine
-__device__ __forceinline__ void bulk_brick(void* dst, const void* src, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 128, [%2];"
-               ::"r"(smem_u32(dst)), "l"(src), "r"(smem_u32(bar))
+// (bytes: a multiple of 16; both addresses 16-B aligned)
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
 
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Loads with a fixed state space.  A list entry comes either from the
+// shared-memory record or from global memory; written as two distinct
+// instructions the compiler cannot fold them into one load of a selected
+// address (a global-only load given a shared address is an address-space
+// fault).
+__device__ __forceinline__ unsigned lds_u16(const void* p) {
+  unsigned short v;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(smem_u32(p)) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned ldg_nc_u16(const uint16_t* p) {
+  unsigned short v;
+  asm volatile("ld.global.nc.u16 %0, [%1];" : "=h"(v) : "l"(p));
+  return v;
 }
 
 // per-bead records shared by the team
@@ -90,9 +108,6 @@ struct __align__(16) BeadPos {  // moved bead; w = ligand type (int bits)
 struct __align__(16) BeadArm {  // lever arm for the torque (Q x) or ligand-frame x (dE/dmat)
   float x, y, z, pad;
 };
-struct __align__(16) BeadList {  // neighbour list: start, count, offset in the flattened team list
-  unsigned start, count, pre, pad;
-};
 
 constexpr int WAIT_LIMIT = 1 << 22;  // try_wait polls before a bulk-copy wait is declared hung
 
@@ -100,9 +115,27 @@ constexpr int WAIT_LIMIT = 1 << 22;  // try_wait polls before a bulk-copy wait i
 // cleared by att_kernel_status()
 __device__ int g_kernel_error = 0;
 
-template <int K>
-__host__ __device__ constexpr size_t warp_smem_bytes() {
-  return (size_t)32 * K * (128 + sizeof(BeadPos) + sizeof(BeadArm) + sizeof(BeadList)) + 16;
+// Debug builds (-DATT_BOUNDS_CHECK) check every computed index against its
+// buffer before the access, skip the access when it is out of range, and
+// record the first failure (check code, index, bound) for att_kernel_debug_info.
+__device__ unsigned long long g_kernel_debug[3] = {0ull, 0ull, 0ull};
+#ifdef ATT_BOUNDS_CHECK
+__device__ __noinline__ void bounds_report(int code, long long a, long long b) {
+  atomicOr(&g_kernel_error, ATT_KERR_BOUNDS);
+  if (atomicCAS(&g_kernel_debug[0], 0ull, (unsigned long long)code) == 0ull) {
+    g_kernel_debug[1] = (unsigned long long)a;
+    g_kernel_debug[2] = (unsigned long long)b;
+  }
+}
+#define ATT_CHECK(cond, code, a, b) ((cond) ? true : (bounds_report((code), (a), (b)), false))
+#else
+#define ATT_CHECK(cond, code, a, b) true
+#endif
+
+// shared memory of one warp: per bead slot a 128-B brick, a neighbour-record
+// slot of rec_slot bytes and two 16-B bead records, then the mbarrier
+__host__ __device__ inline size_t warp_smem_bytes(int K, int rec_slot) {
+  return (size_t)32 * K * (128 + rec_slot + sizeof(BeadPos) + sizeof(BeadArm)) + 16;
 }
 
 template <int S>
@@ -121,39 +154,43 @@ __device__ __forceinline__ int find_segment(const KParams& p, int tile) {
   return lo;
 }
 
-// pair term of one (bead, receptor bead) entry; adds to e and returns dE/dx in g
-__device__ __forceinline__ void pair_term(const KParams& p, const KGrid& G, const BeadPos& bp, const float4& r,
-                                          float& e, float& gx, float& gy, float& gz, bool& hit) {
+// Pair term of one (bead, receptor bead) list entry, branch-free: adds the
+// energy to e and returns dE/dx; a pair that is out of range (beyond the
+// plateau, bad type) adds 0 energy and returns a zero gradient.
+__device__ __forceinline__ void pair_term_masked(const KParams& p, const KGrid& G, const BeadPos& bp,
+                                                 const float4& r, float& e, float& gx, float& gy, float& gz) {
   const float dx = bp.x - r.x, dy = bp.y - r.y, dz = bp.z - r.z;
   const float dsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   const int rt = __float_as_int(r.w);
-  hit = (dsq < G.plateau2) && ((unsigned)rt < (unsigned)G.n_rtypes) && ((unsigned)bp.lt < (unsigned)G.n_ltypes);
-  if (!hit) return;
-  const float4* pp = G.pair + ((long long)bp.lt * G.n_rtypes + rt) * 2;
+  const bool hit =
+      (dsq < G.plateau2) & ((unsigned)rt < (unsigned)G.n_rtypes) & ((unsigned)bp.lt < (unsigned)G.n_ltypes);
+  const int idx = hit ? bp.lt * G.n_rtypes + rt : 0;
+  const float4* pp = G.pair + (long long)idx * 2;
   const float4 p0 = ldg_f4(pp);      // rc, ac, emin, rmin2
   const float4 p1 = ldg_f4(pp + 1);  // ivor, eplat, gplat, rcap2
   const float d2 = fmaxf(dsq, p1.w);
-  const float rr2 = __frcp_rn(d2);
+  float rr2;  // approximate reciprocal (1 ulp): the pair energy carries ~4 ulp
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rr2) : "f"(d2));
   const float rr6 = rr2 * rr2 * rr2;
   const float vlj = fmaf(p0.x, rr2, -p0.y) * rr6;
   const bool near = d2 < p0.w;
   const float en = near ? fmaf(p1.x - 1.f, p0.z, vlj) : p1.x * vlj;
   const float dv = rr6 * rr2 * fmaf(-4.f * p0.x, rr2, 3.f * p0.y);
   float gm = near ? dv : p1.x * dv;
-  if (dsq < p1.w) gm = 0.f;
-  e += en - p1.y;
+  gm = (dsq < p1.w) ? 0.f : gm;
   if (p.grad_mode == ATT_GRAD_REFERENCE) gm = fmaf(-p1.z * G.plateau, rsqrtf(dsq), gm);
-  const float gf = 2.f * gm;
+  const float gf = hit ? 2.f * gm : 0.f;
+  e += hit ? en - p1.y : 0.f;
   gx = gf * dx;
   gy = gf * dy;
   gz = gf * dz;
 }
 
 template <int S, int K, int MODE>
-__global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KParams p) {
+__global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kernel(const __grid_constant__ KParams p) {
   constexpr int P = 32 / S;      // poses per warp
   constexpr int NB = S * K;      // bead slots per pose
-  constexpr int U = 8;           // list entries in flight per lane
+  constexpr int U = 4;           // list entries in flight per lane
   constexpr bool MAT = (MODE == MODE_EVAL_MAT);
   extern __shared__ __align__(128) unsigned char smem_raw[];
 
@@ -162,13 +199,23 @@ __global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KPar
   const int slot = lane / S;
   const int tl = lane % S;
   const int lead = slot * S;
-  unsigned char* wsm = smem_raw + (size_t)warp * warp_smem_bytes<K>();
+  const int RS = p.rec_slot;
+  unsigned char* wsm = smem_raw + (size_t)warp * warp_smem_bytes(K, RS);
   float4* bricks = reinterpret_cast<float4*>(wsm);                          // [32K][8]
-  BeadPos* bpos = reinterpret_cast<BeadPos*>(wsm + 32 * K * 128);
-  BeadArm* barm = reinterpret_cast<BeadArm*>(wsm + 32 * K * (128 + 16));
-  BeadList* blst = reinterpret_cast<BeadList*>(wsm + 32 * K * (128 + 32));
-  uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + 32 * K * (128 + 48));
+  unsigned char* nrec = wsm + 32 * K * 128;                                 // [32K][RS]
+  BeadPos* bpos = reinterpret_cast<BeadPos*>(nrec + 32 * K * RS);
+  BeadArm* barm = reinterpret_cast<BeadArm*>(nrec + 32 * K * (RS + 16));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(nrec + 32 * K * (RS + 32));
   const int tbase = slot * NB;  // this team's first bead record
+
+  // Grid descriptors: copied from the parameters into shared memory with static
+  // parameter offsets only, so that the per-segment grid is picked by a
+  // dynamic index into shared memory (never into the parameter space).
+  __shared__ KGrid s_grid[ATT_MAX_GRIDS];
+#pragma unroll
+  for (int g = 0; g < ATT_MAX_GRIDS; ++g)
+    if (threadIdx.x == g) s_grid[g] = p.grid[g];
+  __syncthreads();
 
   if (lane == 0) {
     mbar_init(bar, 1);
@@ -195,7 +242,7 @@ __global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KPar
     const int local = (tile - __ldg(p.seg_tile + si)) * P + slot;
     const bool valid = local < sg.n_poses;
     const int b = sg.pose0 + (valid ? local : 0);
-    const KGrid& G = p.grid[sg.grid];
+    const KGrid& G = s_grid[sg.grid];
     int lig = sg.lig;
     if (p.pose_lig != nullptr && valid) lig += __ldg(p.pose_lig + b);
     const int loff = __ldg(p.lig_off + lig);
@@ -241,6 +288,11 @@ __global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KPar
     const float dLdE = (MODE == MODE_BWD && valid) ? __ldg(p.dLdE + b) : 0.f;
     int status = 0;
     const int nsteps = (MODE == MODE_MIN) ? p.steps : 0;
+    double bp1 = 1.0, bp2 = 1.0;  // beta1^t, beta2^t of the ADAM bias correction
+    if (MODE == MODE_MIN && p.step0 > 0) {
+      bp1 = pow((double)p.b1, (double)p.step0);
+      bp2 = pow((double)p.b2, (double)p.step0);
+    }
 
     for (int s = 0; s <= nsteps; ++s) {
       // ---------------- pose -> rotation Q (column form) and translation t
@@ -252,16 +304,19 @@ __global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KPar
         q02 = mat[6]; q12 = mat[7]; q22 = mat[8];
         tx = mat[9]; ty = mat[10]; tz = mat[11];
       } else {
-        const float phi = __shfl_sync(0xffffffffu, my_x, lead + 0);
-        const float psi = __shfl_sync(0xffffffffu, my_x, lead + 1);
-        const float th = __shfl_sync(0xffffffffu, my_x, lead + 2);
+        // team lanes 0..2 hold the three angles: one sincosf per lane, then
+        // broadcast (one sincos instruction stream per warp instead of three)
+        float my_s, my_c;
+        sincosf(my_x, &my_s, &my_c);
+        sphi = __shfl_sync(0xffffffffu, my_s, lead + 0);
+        cphi = __shfl_sync(0xffffffffu, my_c, lead + 0);
+        spsi = __shfl_sync(0xffffffffu, my_s, lead + 1);
+        cpsi = __shfl_sync(0xffffffffu, my_c, lead + 1);
+        const float sth = __shfl_sync(0xffffffffu, my_s, lead + 2);
+        const float cth = __shfl_sync(0xffffffffu, my_c, lead + 2);
         tx = __shfl_sync(0xffffffffu, my_x, lead + 3);
         ty = __shfl_sync(0xffffffffu, my_x, lead + 4);
         tz = __shfl_sync(0xffffffffu, my_x, lead + 5);
-        float sth, cth;
-        sincosf(phi, &sphi, &cphi);
-        sincosf(psi, &spsi, &cpsi);
-        sincosf(th, &sth, &cth);
         // Q = Rz(phi) Ry(psi) Rz(-theta)
         q00 = cphi * cpsi * cth + sphi * sth;
         q01 = cphi * cpsi * sth - sphi * cth;
@@ -289,8 +344,6 @@ __global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KPar
       bool use[K], outer_k[K];
       long long bidx[K];  // brick index
       long long nvox[K];  // nearest inner grid point for the list lookup, -1 = none
-      uint2 hdr[K];
-      unsigned nuse = 0;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         const int i = tl + k * S;
@@ -341,11 +394,12 @@ __global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KPar
                           biz[k]
                     : 0;
         nvox[k] = -1;
-        if (inn && G.nb_hdr != nullptr && lt < G.n_ltypes) {
+        if (inn && G.nb_rec != nullptr && lt < G.n_ltypes) {
           const int nx = (int)floorf(vx + 0.5f), my = (int)floorf(vy + 0.5f), mz = (int)floorf(vz + 0.5f);
           nvox[k] = ((long long)nx * G.dy + my) * G.dz + mz;
         }
-        nuse += __popc(__ballot_sync(0xffffffffu, u));
+        if (use[k] && !ATT_CHECK(bidx[k] >= 0 && bidx[k] < G.n_bricks, 1, bidx[k], G.n_bricks)) use[k] = false;
+        if (nvox[k] >= 0 && !ATT_CHECK(nvox[k] < G.n_vox, 2, nvox[k], G.n_vox)) nvox[k] = -1;
         // records for the team (generic-proxy writes)
         if (live) {
           BeadPos bp;
@@ -358,121 +412,28 @@ __global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KPar
           barm[tbase + i] = ba;
         }
       }
-      // the mbarrier phase completes when lane 0 has arrived and all
-      // nuse * 128 bytes have landed (the copies may finish before the arrive)
-      if (lane == 0) mbar_arrive_expect_tx(bar, nuse * 128u);
+      // one bulk copy per brick and per neighbour record; the mbarrier phase
+      // completes when lane 0 has arrived and all bytes have landed (copies
+      // may finish before the arrive)
+      unsigned my_bytes = 0;
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        my_bytes += (use[k] ? 128u : 0u) + (nvox[k] >= 0 ? (unsigned)G.nb_rec_bytes : 0u);
+      const unsigned warp_bytes = __reduce_add_sync(0xffffffffu, my_bytes);
+      if (lane == 0) mbar_arrive_expect_tx(bar, warp_bytes);
       __syncwarp();
 #pragma unroll
       for (int k = 0; k < K; ++k) {
+        const int sk = tbase + tl + k * S;
         if (use[k]) {
-          bulk_brick(bricks + (size_t)(tbase + tl + k * S) * 8, G.bricks + bidx[k] * 8, bar);
+          bulk_copy(bricks + (size_t)sk * 8, G.bricks + bidx[k] * 8, 128u, bar);
           if (MODE == MODE_MIN) c_grid += 1;
         }
-      }
-      // neighbour-list headers (L2-resident)
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        hdr[k] = make_uint2(0u, 0u);
         if (nvox[k] >= 0) {
-          hdr[k] = ldg_u2(G.nb_hdr + nvox[k]);
+          bulk_copy(nrec + (size_t)sk * RS, G.nb_rec + nvox[k] * G.nb_rec_bytes, (unsigned)G.nb_rec_bytes, bar);
           if (MODE == MODE_MIN) c_look += 1;
         }
       }
-
-      // ---------------- phase B: flattened list offsets (team scan in bead order)
-      unsigned carry = 0;
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const unsigned c = hdr[k].y;
-        unsigned inc = c;
-#pragma unroll
-        for (int off = 1; off < S; off <<= 1) {
-          const unsigned t = __shfl_up_sync(0xffffffffu, inc, off, S);
-          if (tl >= off) inc += t;
-        }
-        const int i = tl + k * S;
-        if (i < N) {
-          BeadList bl;
-          bl.start = hdr[k].x;
-          bl.count = c;
-          bl.pre = carry + inc - c;
-          bl.pad = 0u;
-          blst[tbase + i] = bl;
-        }
-        carry += __shfl_sync(0xffffffffu, inc, lead + S - 1);
-      }
-      const unsigned total = carry;
-      __syncwarp();
-
-      // ---------------- phase C: the team's flattened neighbour list
-      if (total > 0) {
-        const unsigned chunk = (total + S - 1) / S;
-        unsigned e = tl * chunk;
-        const unsigned e_end = min(total, e + chunk);
-        // bead holding entry e: the last bead whose offset is <= e
-        int bi = 0;
-        if (e < e_end) {
-          int lo = 0, hi = N - 1;
-          while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (blst[tbase + mid].pre <= e) lo = mid; else hi = mid - 1;
-          }
-          bi = lo;
-        }
-        if (MODE == MODE_MIN) c_ent += (e < e_end) ? (e_end - e) : 0u;
-        while (e < e_end) {
-          unsigned jj[U];
-          int bb[U];
-#pragma unroll
-          for (int m = 0; m < U; ++m) {
-            jj[m] = ATT_NB_EMPTY;
-            bb[m] = bi;
-            if (e + m < e_end) {
-              BeadList bl = blst[tbase + bi];
-              while (e + m >= bl.pre + bl.count) {
-                ++bi;
-                bl = blst[tbase + bi];
-              }
-              bb[m] = bi;
-              jj[m] = ldg_u16(G.nb_list + bl.start + (e + m - bl.pre));
-            }
-          }
-#pragma unroll
-          for (int h = 0; h < U; h += 4) {
-            float4 rr[4];
-#pragma unroll
-            for (int m = 0; m < 4; ++m) {
-              const unsigned j = jj[h + m];
-              rr[m] = (j < (unsigned)G.n_rec) ? ldg_f4(G.rec + j) : make_float4(1e30f, 1e30f, 1e30f, 0.f);
-            }
-#pragma unroll
-            for (int m = 0; m < 4; ++m) {
-              const BeadPos bp = bpos[tbase + bb[h + m]];
-              float gx, gy, gz;
-              bool hit;
-              pair_term(p, G, bp, rr[m], acc_e, gx, gy, gz, hit);
-              if (hit) {
-                const BeadArm ba = barm[tbase + bb[h + m]];
-                acc_gx += gx;
-                acc_gy += gy;
-                acc_gz += gz;
-                if (MAT) {
-                  acc_t[0] = fmaf(ba.x, gx, acc_t[0]); acc_t[1] = fmaf(ba.x, gy, acc_t[1]); acc_t[2] = fmaf(ba.x, gz, acc_t[2]);
-                  acc_t[3] = fmaf(ba.y, gx, acc_t[3]); acc_t[4] = fmaf(ba.y, gy, acc_t[4]); acc_t[5] = fmaf(ba.y, gz, acc_t[5]);
-                  acc_t[6] = fmaf(ba.z, gx, acc_t[6]); acc_t[7] = fmaf(ba.z, gy, acc_t[7]); acc_t[8] = fmaf(ba.z, gz, acc_t[8]);
-                } else {
-                  acc_t[0] = fmaf(ba.y, gz, fmaf(-ba.z, gy, acc_t[0]));
-                  acc_t[1] = fmaf(ba.z, gx, fmaf(-ba.x, gz, acc_t[1]));
-                  acc_t[2] = fmaf(ba.x, gy, fmaf(-ba.y, gx, acc_t[2]));
-                }
-              }
-            }
-          }
-          e += U;
-        }
-      }
-
-      // ---------------- phase D: grid term from the bricks in shared memory
       {
         bool done = false;
         for (int it = 0; it < WAIT_LIMIT && !done; ++it) done = mbar_try_wait(bar, parity);
@@ -482,6 +443,82 @@ __global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KPar
         }
         parity ^= 1u;
       }
+
+      // ---------------- phase C: neighbour lists, bead-major: each owner lane
+      // walks its own beads' lists (inline entries from the shared-memory
+      // record, the rest from the CSR overflow) with the bead in registers,
+      // U entries in flight, and one torque cross product per bead
+      const unsigned ninl = (unsigned)G.nb_inline;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int i = tl + k * S;
+        const unsigned char* rk = nrec + (size_t)(tbase + i) * RS;
+        const unsigned cnt = (nvox[k] >= 0) ? *reinterpret_cast<const uint16_t*>(rk + 4) : 0u;
+        if (MODE == MODE_MIN) c_ent += cnt;
+        if (cnt == 0) continue;
+        const unsigned ovf = *reinterpret_cast<const unsigned*>(rk);
+#ifdef ATT_BOUNDS_CHECK
+        if (cnt > ninl && !ATT_CHECK((long long)ovf - ninl + cnt <= G.n_list, 6, ovf, cnt)) continue;
+#endif
+        const uint16_t* inl = reinterpret_cast<const uint16_t*>(rk + 6);
+        const BeadPos bp = bpos[tbase + i];
+        float ge = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+        for (unsigned li = 0; li < cnt; li += U) {
+          unsigned jj[U];
+#pragma unroll
+          for (int m = 0; m < U; ++m) {
+            const unsigned idx = li + m;
+#ifdef ATT_BOUNDS_CHECK
+            unsigned j = ATT_NB_EMPTY;
+            if (idx < cnt) {
+              if (idx < ninl) {
+                j = lds_u16(inl + idx);
+              } else {
+                const long long oi = (long long)ovf + (long long)(idx - ninl);
+                if (ATT_CHECK(oi >= 0 && oi < G.n_list, 3, oi, G.n_list)) j = ldg_u16(G.nb_list + oi);
+              }
+              if (j != ATT_NB_EMPTY && !ATT_CHECK(j < (unsigned)G.n_rec, 4, j, G.n_rec)) j = ATT_NB_EMPTY;
+            }
+            jj[m] = j;
+#else
+            unsigned j = ATT_NB_EMPTY;
+            if (idx < cnt) {
+              if (idx < ninl) j = lds_u16(inl + idx);
+              else j = ldg_nc_u16(G.nb_list + (ovf + (idx - ninl)));
+            }
+            jj[m] = j;
+#endif
+          }
+          float4 rr[U];
+#pragma unroll
+          for (int m = 0; m < U; ++m)
+            rr[m] = (jj[m] < (unsigned)G.n_rec) ? ldg_f4(G.rec + jj[m]) : make_float4(1e15f, 1e15f, 1e15f, 0.f);
+#pragma unroll
+          for (int m = 0; m < U; ++m) {
+            float px, py, pz;
+            pair_term_masked(p, G, bp, rr[m], ge, px, py, pz);
+            gx += px;
+            gy += py;
+            gz += pz;
+          }
+        }
+        const BeadArm ba = barm[tbase + i];
+        acc_e += ge;
+        acc_gx += gx;
+        acc_gy += gy;
+        acc_gz += gz;
+        if (MAT) {
+          acc_t[0] = fmaf(ba.x, gx, acc_t[0]); acc_t[1] = fmaf(ba.x, gy, acc_t[1]); acc_t[2] = fmaf(ba.x, gz, acc_t[2]);
+          acc_t[3] = fmaf(ba.y, gx, acc_t[3]); acc_t[4] = fmaf(ba.y, gy, acc_t[4]); acc_t[5] = fmaf(ba.y, gz, acc_t[5]);
+          acc_t[6] = fmaf(ba.z, gx, acc_t[6]); acc_t[7] = fmaf(ba.z, gy, acc_t[7]); acc_t[8] = fmaf(ba.z, gz, acc_t[8]);
+        } else {
+          acc_t[0] = fmaf(ba.y, gz, fmaf(-ba.z, gy, acc_t[0]));
+          acc_t[1] = fmaf(ba.z, gx, fmaf(-ba.x, gz, acc_t[1]));
+          acc_t[2] = fmaf(ba.x, gy, fmaf(-ba.y, gx, acc_t[2]));
+        }
+      }
+
+      // ---------------- phase D: grid term from the bricks in shared memory
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (use[k]) {
@@ -516,7 +553,8 @@ __global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KPar
                 const int nz = outer_k[k] ? G.dz2 : G.dz;
                 const long long off =
                     ((((long long)brick_gt[k] * nx + bix[k] + cx) * ny + biy[k] + cy) * (long long)nz + biz[k] + cz) * 4;
-                atomicAdd(dg + off, dLdE * w);
+                const long long lim = outer_k[k] ? p.n_dgrid_outer : p.n_dgrid_inner;
+                if (ATT_CHECK(off >= 0 && off + 4 <= lim, 5, off, lim)) atomicAdd(dg + off, dLdE * w);
               }
             }
           }
@@ -597,14 +635,16 @@ __global__ void __launch_bounds__(128) score_kernel(const __grid_constant__ KPar
       // ---- fused ADAM step on lanes 0..5 (optax.adam form)
       const bool ok = isfinite(gtx) & isfinite(gty) & isfinite(gtz) & isfinite(gphi) & isfinite(gpsi) &
                       isfinite(gth);
+      // beta^t as running double products (t counts skipped steps too)
+      bp1 *= (double)p.b1;
+      bp2 *= (double)p.b2;
       if (!ok) {
         status |= ATT_STATUS_NONFINITE_GRAD;
       } else if (tl < 6) {
-        const float t = (float)(p.step0 + s + 1);
         my_m = fmaf(p.b1, my_m, (1.f - p.b1) * gk);
         my_v = fmaf(p.b2, my_v, (1.f - p.b2) * gk * gk);
-        const float mh = my_m / (1.f - powf(p.b1, t));
-        const float vh = my_v / (1.f - powf(p.b2, t));
+        const float mh = my_m / (float)(1.0 - bp1);
+        const float vh = my_v / (float)(1.0 - bp2);
         const float lr = (tl < 3) ? p.lr_rot : p.lr_trans;
         my_x -= lr * mh / (sqrtf(vh) + p.eps);
       }
@@ -655,16 +695,6 @@ struct KernelTable {
   }
 };
 
-static size_t smem_per_warp(int K) {
-  switch (K) {
-    case 1: return warp_smem_bytes<1>();
-    case 2: return warp_smem_bytes<2>();
-    case 4: return warp_smem_bytes<4>();
-    case 8: return warp_smem_bytes<8>();
-  }
-  return 0;
-}
-
 static const void* kernel_of(int mode, int S, int K) {
   switch (mode) {
     case MODE_EVAL: return KernelTable<MODE_EVAL>::get(S, K);
@@ -682,12 +712,14 @@ int beads_per_lane(int S, int max_beads) {
   return K <= ATT_MAX_BEADS_PER_LANE ? K : ATT_MAX_BEADS_PER_LANE;  // larger ligands run in chunks
 }
 
-size_t score_smem_bytes(int K, int threads) { return smem_per_warp(K) * (size_t)(threads / 32); }
+size_t score_smem_bytes(int K, int threads, int rec_slot) {
+  return warp_smem_bytes(K, rec_slot) * (size_t)(threads / 32);
+}
 
 cudaError_t launch_score(const KParams& p, int mode, int S, int K, int blocks, int threads, cudaStream_t st) {
   const void* k = kernel_of(mode, S, K);
   if (k == nullptr) return cudaErrorInvalidValue;
-  const size_t smem = score_smem_bytes(K, threads);
+  const size_t smem = score_smem_bytes(K, threads, p.rec_slot);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   void* args[] = {const_cast<KParams*>(&p)};
@@ -705,10 +737,22 @@ cudaError_t kernel_status(int* out, int clear, cudaStream_t st) {
   return e;
 }
 
-cudaError_t occupancy_blocks(int mode, int S, int K, int threads, int* blocks_per_sm) {
+cudaError_t kernel_debug_info(unsigned long long* out3, int clear, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyFromSymbolAsync(out3, g_kernel_debug, 3 * sizeof(unsigned long long), 0,
+                                            cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && clear) {
+    const unsigned long long zero[3] = {0ull, 0ull, 0ull};
+    e = cudaMemcpyToSymbolAsync(g_kernel_debug, zero, sizeof(zero), 0, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  return e;
+}
+
+cudaError_t occupancy_blocks(int mode, int S, int K, int threads, int rec_slot, int* blocks_per_sm) {
   const void* k = kernel_of(mode, S, K);
   if (k == nullptr) return cudaErrorInvalidValue;
-  const size_t smem = score_smem_bytes(K, threads);
+  const size_t smem = score_smem_bytes(K, threads, rec_slot);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k, threads, smem);

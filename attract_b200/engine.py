@@ -58,7 +58,7 @@ class AdamOptions:
 @dataclass
 class LaunchShape:
     lanes_per_pose: int = 8   # 8 / 16 / 32 lanes per pose = 4 / 2 / 1 poses per warp
-    block_threads: int = 128  # 32, 64, 96 or 128
+    block_threads: int = 0    # 32, 64, 96 or 128; 0 = the largest that fits in shared memory
     blocks: int = 0           # persistent CTAs; 0 = fill the GPU
 
     def to_c(self) -> _lib.AttLaunchCfg:

@@ -125,7 +125,31 @@ class Grid:
             shift_plateau = bricks is not None
         self.shift_plateau = shift_plateau
         self.pair = torch.from_numpy(ff.pair_table(geom.plateau, shift_plateau)).to(self.device)
+        # versions of the dense grids the bricks were packed from (autograd.py)
+        self._packed_version = (None if inner is None else inner._version,
+                                None if outer is None else outer._version)
+        self.nb_rec = None
+        self.nb_rec_bytes = 0
+        if nb_hdr is not None:
+            self._pack_records()
         self._att = None
+
+    def _pack_records(self, rec_bytes: int | None = None):
+        """Fixed-size neighbour records (one bulk copy per bead and step): the
+        smallest of 32/64/128 bytes whose inline entries hold 99 % of the
+        non-empty lists; longer lists continue in the CSR list."""
+        counts = self.nb_hdr[:, 1]
+        if rec_bytes is None:
+            nz = counts[counts > 0].to(torch.float32)
+            q = float(torch.quantile(nz[: 1 << 24], 0.99).item()) if nz.numel() else 0.0
+            rec_bytes = next((b for b in (32, 64, 128) if (b - 6) // 2 >= q), 128)
+        self.nb_rec_bytes = rec_bytes
+        self.nb_rec = torch.empty(self.geom.n_voxels * rec_bytes, dtype=torch.uint8, device=self.device)
+        with torch.cuda.device(self.device):
+            st = torch.cuda.current_stream(self.device).cuda_stream
+            _lib.check(_lib.load().att_nbgrid_pack_records(_lib.ptr(self.nb_hdr), _lib.ptr(self.nb_list),
+                                                           self.geom.n_voxels, rec_bytes, _lib.ptr(self.nb_rec),
+                                                           st), "att_nbgrid_pack_records")
 
     # ------------------------------------------------------------------ C view
     def att(self) -> _lib.AttGrid:
@@ -143,6 +167,8 @@ class Grid:
             a.n_rtypes = self.ff.n_rtypes
             a.n_ltypes = self.ff.n_ltypes
             a.pair = _lib.ptr(self.pair)
+            a.nb_rec = _lib.ptr(self.nb_rec)
+            a.nb_rec_bytes = self.nb_rec_bytes
             self._att = a
         return self._att
 
@@ -154,7 +180,8 @@ class Grid:
 
     def nbytes(self) -> int:
         return sum(t.numel() * t.element_size() for t in (self.bricks, self.nb_hdr, self.nb_list, self.rec,
-                                                            self.pair, self.inner, self.outer) if t is not None)
+                                                            self.pair, self.inner, self.outer, self.nb_rec)
+                   if t is not None)
 
     # ------------------------------------------------------------ constructors
     @classmethod

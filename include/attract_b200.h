@@ -54,6 +54,7 @@ extern "C" {
 
 /* device-wide kernel error word (att_kernel_status) */
 #define ATT_KERR_COPY_TIMEOUT 1 /* a warp gave up waiting for its grid-brick bulk copies and returned */
+#define ATT_KERR_BOUNDS 2       /* (ATT_BOUNDS_CHECK builds) an index failed its check; the access was skipped */
 
 /* A pose is served by lanes_per_pose lanes holding up to 8 beads each; a
    ligand with more than 8 * lanes_per_pose beads is evaluated in chunks of that
@@ -79,16 +80,23 @@ typedef struct AttGrid {
                                   NULL = no potential grid (neighbour grid only) */
   long long n_inner_bricks;    /* (dim[0]-1)(dim[1]-1)(dim[2]-1) */
   long long n_outer_bricks;    /* (dim2[0]-1)(dim2[1]-1)(dim2[2]-1), 0 = no outer grid */
-  const uint32_t* nb_hdr;      /* [dim0*dim1*dim2][2] = {start, count} per inner grid point; NULL = none */
+  const uint32_t* nb_hdr;      /* [dim0*dim1*dim2][2] = {start, count} per inner grid point (CSR);
+                                  NULL = no neighbour grid */
   const uint16_t* nb_list;     /* receptor bead index per entry (ATT_NB_EMPTY skipped) */
   long long n_nb_entries;
   const float* rec;            /* [n_rec][4] x, y, z, receptor type (as an int32 bit pattern) */
   int n_rec;
   int n_rtypes;                /* receptor types in the pair table */
   int n_ltypes;                /* ligand types in the pair table */
-  int pad_;
+  int nb_rec_bytes;            /* 32, 64 or 128: size of one neighbour record (below) */
   const float* pair;           /* [n_ltypes][n_rtypes][8]: rc, ac, emin, rmin2, ivor, eplat, gplat, rcap2 */
+  const void* nb_rec;          /* [dim0*dim1*dim2] neighbour records, 16-B aligned (att_nbgrid_pack_records):
+                                  u32 overflow index into nb_list, u16 count, then the first
+                                  (nb_rec_bytes - 6) / 2 entries inline; required with nb_hdr */
 } AttGrid;
+
+/* Inline entries of a neighbour record of `bytes` bytes. */
+#define ATT_NB_INLINE(bytes) (((bytes) - 6) / 2)
 
 /* Ligands: all beads of all ligands concatenated. */
 typedef struct AttLigands {
@@ -124,7 +132,7 @@ typedef struct AttAdamCfg {
 /* Launch shape; zeros pick the defaults / autotuned values. */
 typedef struct AttLaunchCfg {
   int lanes_per_pose;   /* 8, 16 or 32 (poses per warp = 32 / lanes_per_pose) */
-  int block_threads;    /* 32, 64, 96 or 128 (0 = 128) */
+  int block_threads;    /* 32, 64, 96 or 128 (0 = the largest whose shared memory fits) */
   int blocks;           /* persistent CTAs (att_minimise), 0 = fill the GPU */
   int pad_;
 } AttLaunchCfg;
@@ -197,6 +205,16 @@ int att_nbgrid_count(const AttGridGeom* geom, const float* rec_dev, int n_rec, f
 int att_nbgrid_fill(const AttGridGeom* geom, const float* rec_dev, int n_rec, float radius,
                     const uint32_t* hdr_dev, uint16_t* list_dev, void* stream);
 
+/* Fixed-size neighbour records from the CSR lists: record v holds
+   {overflow index = start + inline, count, first `inline` entries (rest
+   ATT_NB_EMPTY)}; entries beyond the inline ones stay in the CSR list, which
+   the kernels keep reading.  One record is one bulk copy per bead and step.
+   records_dev: n_voxels * rec_bytes bytes, 16-B aligned; rec_bytes 32/64/128.
+   (No counterpart in the reference: a layout of the neighbour grid of
+   read_grid2.py:113-124 for the B200 kernels.) */
+int att_nbgrid_pack_records(const uint32_t* hdr_dev, const uint16_t* list_dev, long long n_voxels,
+                            int rec_bytes, void* records_dev, void* stream);
+
 /* att_nbgrid_count without a caller workspace.  No counterpart in the
    reference (its neighbour lists come from a KD-tree on the host).
    Some callers of this library cannot allocate device memory: a plugin that
@@ -221,6 +239,11 @@ int att_nbgrid_count_noalloc(const AttGridGeom* geom, const float* rec_dev, int 
    non-zero word means some warp stopped early and its poses' outputs are stale.
    (No counterpart in the reference: JAX has no device-side waits.) */
 int att_kernel_status(int* error_word, int clear, void* stream);
+
+/* Debug builds (-DATT_BOUNDS_CHECK): the first failed index check of the
+   scoring kernels as {check code, index, bound} (zeros if none, and always in
+   regular builds); cleared if `clear`; synchronises `stream`. */
+int att_kernel_debug_info(unsigned long long* info3, int clear, void* stream);
 
 #ifdef __cplusplus
 }

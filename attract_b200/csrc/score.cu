@@ -134,8 +134,9 @@ __device__ __noinline__ void bounds_report(int code, long long a, long long b) {
 
 // shared memory of one warp: per bead slot a 128-B brick, a neighbour-record
 // slot of rec_slot bytes and two 16-B bead records, then the mbarrier
+__host__ __device__ inline int rec_stride(int rec_slot) { return rec_slot ? rec_slot + 16 : 0; }
 __host__ __device__ inline size_t warp_smem_bytes(int K, int rec_slot) {
-  return (size_t)32 * K * (128 + rec_slot + sizeof(BeadPos) + sizeof(BeadArm)) + 16;
+  return (size_t)32 * K * (128 + rec_stride(rec_slot) + sizeof(BeadPos) + sizeof(BeadArm)) + 16;
 }
 
 template <int S>
@@ -199,8 +200,8 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
   const int slot = lane / S;
   const int tl = lane % S;
   const int lead = slot * S;
-  const int RS = p.rec_slot;
-  unsigned char* wsm = smem_raw + (size_t)warp * warp_smem_bytes(K, RS);
+  const int RS = rec_stride(p.rec_slot);
+  unsigned char* wsm = smem_raw + (size_t)warp * warp_smem_bytes(K, p.rec_slot);
   float4* bricks = reinterpret_cast<float4*>(wsm);                          // [32K][8]
   unsigned char* nrec = wsm + 32 * K * 128;                                 // [32K][RS]
   BeadPos* bpos = reinterpret_cast<BeadPos*>(nrec + 32 * K * RS);

@@ -44,7 +44,8 @@ class AttLigands(C.Structure):
 
 
 class AttSegment(C.Structure):
-    _fields_ = [("grid", C.c_int), ("lig", C.c_int), ("pose0", C.c_int), ("n_poses", C.c_int)]
+    _fields_ = [("grid", C.c_int), ("lig", C.c_int), ("pose0", C.c_int), ("n_poses", C.c_int),
+                ("step0", C.c_int), ("pad_", C.c_int * 3)]
 
 
 class AttEvalCfg(C.Structure):

@@ -290,9 +290,10 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
     int status = 0;
     const int nsteps = (MODE == MODE_MIN) ? p.steps : 0;
     double bp1 = 1.0, bp2 = 1.0;  // beta1^t, beta2^t of the ADAM bias correction
-    if (MODE == MODE_MIN && p.step0 > 0) {
-      bp1 = pow((double)p.b1, (double)p.step0);
-      bp2 = pow((double)p.b2, (double)p.step0);
+    const int step0 = p.step0 + sg.step0;
+    if (MODE == MODE_MIN && step0 > 0) {
+      bp1 = pow((double)p.b1, (double)step0);
+      bp2 = pow((double)p.b2, (double)step0);
     }
 
     for (int s = 0; s <= nsteps; ++s) {

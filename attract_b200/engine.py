@@ -75,6 +75,8 @@ class Segment(NamedTuple):
     grid: int
     lig: int
     n_poses: int
+    step0: int = 0            # ADAM steps already taken by these poses' state
+    pose0: int | None = None  # first pose in the pose array (None: packed in segment order)
 
 
 def _stream(stream):
@@ -89,7 +91,9 @@ class Workload:
     """Device tables for launches over ``segments`` (see module docstring)."""
 
     def __init__(self, grids: Sequence[Grid], ligands: LigandSet, segments: Sequence[Segment],
-                 lanes_per_pose: int = 8, device=None):
+                 lanes_per_pose: int = 8, device=None, n_poses: int | None = None):
+        """``n_poses``: size of the pose array when segments give explicit
+        ``pose0`` offsets (a pose pool); otherwise segments are packed in order."""
         if not 1 <= len(grids) <= _lib.ATT_MAX_GRIDS:
             raise ValueError(f"1..{_lib.ATT_MAX_GRIDS} grids per launch, got {len(grids)}")
         if lanes_per_pose not in (8, 16, 32):
@@ -100,10 +104,19 @@ class Workload:
         self.segments = [Segment(*s) for s in segments]
         if not self.segments:
             raise ValueError("no segments")
+        explicit = [s.pose0 is not None for s in self.segments]
+        if any(explicit) and not (all(explicit) and n_poses is not None):
+            raise ValueError("explicit pose0 needs pose0 on every segment and n_poses")
         self.lanes = lanes_per_pose
         P = 32 // lanes_per_pose
         rows, tiles, pose0 = [], [0], 0
         for s in self.segments:
+            if s.pose0 is not None:
+                if s.pose0 < 0 or s.pose0 + s.n_poses > n_poses:
+                    raise ValueError(f"segment {s} lies outside the {n_poses}-pose array")
+                pose0 = s.pose0
+            if s.step0 < 0:
+                raise ValueError("negative step0")
             if not (0 <= s.grid < len(grids)) or not (0 <= s.lig < len(ligands)):
                 raise ValueError(f"segment {s} refers to a missing grid or ligand")
             if s.n_poses < 0:
@@ -114,10 +127,11 @@ class Workload:
                 raise ValueError(f"ligand {s.lig}: grid type {gt.max()} >= grid {s.grid}'s {g.geom.n_types} slots")
             if lt.max() >= g.ff.n_ltypes:
                 raise ValueError(f"ligand {s.lig}: ligand type {lt.max()} outside grid {s.grid}'s force field")
-            rows.append((s.grid, s.lig, pose0, s.n_poses))
+            rows.append((s.grid, s.lig, pose0, s.n_poses, s.step0, 0, 0, 0))
             tiles.append(tiles[-1] + (s.n_poses + P - 1) // P)
             pose0 += s.n_poses
-        self.n_poses = pose0
+        self.n_poses = pose0 if n_poses is None else int(n_poses)
+        self._pool = n_poses is not None
         self.n_tiles = tiles[-1]
         self.pose0 = [r[2] for r in rows]
         self.segs = torch.tensor(rows, dtype=torch.int32, device=self.device)
@@ -129,7 +143,8 @@ class Workload:
     def with_lanes(self, lanes_per_pose: int) -> "Workload":
         if lanes_per_pose == self.lanes:
             return self
-        return Workload(self.grids, self.ligands, self.segments, lanes_per_pose, self.device)
+        return Workload(self.grids, self.ligands, self.segments, lanes_per_pose, self.device,
+                        self.n_poses if self._pool else None)
 
     def bead_evals(self, evals_per_pose: int) -> int:
         return int(sum(self.ligands.sizes[s.lig] * s.n_poses for s in self.segments)) * evals_per_pose

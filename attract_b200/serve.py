@@ -1,0 +1,233 @@
+"""Continuous-batching docking server with receptor grids resident in HBM.
+
+Requests (receptor, ligand, poses) are admitted while the pose pool and the
+HBM budget allow, minimised in *rounds*: one persistent kernel launch
+advances every admitted request by ``round_steps`` ADAM steps, whatever its
+receptor, ligand size or progress (each request is one segment of the launch
+with its own ADAM step offset, its pose / ADAM state living in a slice of the
+pool).  A request that arrives while others are on the GPU joins at the next
+round; a finished request leaves and frees its slice.  The result of a
+request does not depend on what it was batched with: per-pose arithmetic is
+independent of the other poses of a launch.
+
+Latency is wall-clock from ``submit`` to completion; ``stats()`` reports
+p50/p99 latency and sustained poses/s.
+"""
+from __future__ import annotations
+
+import bisect
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .engine import AdamOptions, EvalOptions, LaunchShape, Segment, Workload, minimise, MinimiseScratch
+from .ligand import LigandSet
+
+POSE_BYTES = 4 * (6 + 12 + 1 + 1)  # pose, ADAM state, energy, status
+
+
+@dataclass
+class Request:
+    receptor: int
+    ligand: tuple            # (xyz [N,3], gtype [N], ltype [N] or None)
+    poses: np.ndarray        # [n, 6]
+    rid: int = -1
+    arrival: float = 0.0
+    admitted: float = 0.0
+    finished: float = 0.0
+    slot0: int = -1
+    step: int = 0
+    result_poses: np.ndarray | None = None
+    result_energies: np.ndarray | None = None
+    result_status: np.ndarray | None = None
+
+    @property
+    def n(self) -> int:
+        return len(self.poses)
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+class PosePool:
+    """First-fit allocator of contiguous pose ranges in [0, capacity)."""
+
+    def __init__(self, capacity: int):
+        self.capacity = capacity
+        self.free = [(0, capacity)]  # sorted (start, length)
+
+    def alloc(self, n: int) -> int:
+        for i, (s, ln) in enumerate(self.free):
+            if ln >= n:
+                if ln == n:
+                    self.free.pop(i)
+                else:
+                    self.free[i] = (s + n, ln - n)
+                return s
+        return -1
+
+    def release(self, s: int, n: int):
+        i = bisect.bisect_left(self.free, (s, 0))
+        self.free.insert(i, (s, n))
+        merged = []
+        for a, ln in self.free:
+            if merged and merged[-1][0] + merged[-1][1] == a:
+                merged[-1] = (merged[-1][0], merged[-1][1] + ln)
+            else:
+                merged.append((a, ln))
+        self.free = merged
+
+    @property
+    def used(self) -> int:
+        return self.capacity - sum(ln for _, ln in self.free)
+
+
+class DockingServer:
+    def __init__(self, grids, steps: int = 200, round_steps: int = 25, max_inflight_poses: int = 1_000_000,
+                 hbm_budget_bytes: float = 150e9, adam: AdamOptions | None = None, opts: EvalOptions | None = None,
+                 launch: LaunchShape | None = None, device=None):
+        if steps % round_steps:
+            raise ValueError("steps must be a multiple of round_steps")
+        if len(grids) > 8:
+            raise ValueError("at most 8 resident receptors per launch")
+        self.grids = list(grids)
+        self.device = self.grids[0].device if device is None else torch.device(device)
+        self.steps, self.round_steps = steps, round_steps
+        self.adam = adam or AdamOptions()
+        self.opts = opts or EvalOptions()
+        self.launch = launch or LaunchShape(lanes_per_pose=32)
+        grid_bytes = sum(g.nbytes() for g in self.grids)
+        cap = int(min(max_inflight_poses, max(0.0, hbm_budget_bytes - grid_bytes) // POSE_BYTES))
+        if cap <= 0:
+            raise ValueError("the HBM budget does not cover the resident grids")
+        self.capacity = cap
+        self.hbm_budget = hbm_budget_bytes
+        self.grid_bytes = grid_bytes
+        self.pool = PosePool(cap)
+        d = self.device
+        self.pose = torch.zeros((cap, 6), dtype=torch.float32, device=d)
+        self.state = torch.zeros((cap, 12), dtype=torch.float32, device=d)
+        self.scratch = MinimiseScratch(cap, d)
+        self.pending: deque[Request] = deque()
+        self.active: list[Request] = []
+        self.done: list[Request] = []
+        self._ligset = None
+        self._ligset_key = None
+        self._next_rid = 0
+        self.rounds = 0
+        self.gpu_ms = 0.0
+        self.t0 = time.perf_counter()
+
+    # ------------------------------------------------------------------ API
+    def submit(self, req: Request, now: float | None = None) -> Request:
+        if not 0 <= req.receptor < len(self.grids):
+            raise ValueError("unknown receptor")
+        if req.n > self.capacity:
+            raise ValueError(f"request of {req.n} poses exceeds the pool of {self.capacity}")
+        req.rid = self._next_rid
+        self._next_rid += 1
+        req.arrival = time.perf_counter() if now is None else now
+        self.pending.append(req)
+        return req
+
+    def idle(self) -> bool:
+        return not self.pending and not self.active
+
+    def run_until_idle(self):
+        while not self.idle():
+            self.round()
+
+    def stats(self, since: float | None = None) -> dict:
+        reqs = [r for r in self.done if since is None or r.arrival >= since]
+        lat = np.array([r.latency for r in reqs]) if reqs else np.zeros(0)
+        poses = int(sum(r.n for r in reqs))
+        span = (max(r.finished for r in reqs) - min(r.arrival for r in reqs)) if reqs else 0.0
+        return {"requests": len(reqs), "poses": poses,
+                "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+                "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+                "poses_per_s": poses / span if span > 0 else None,
+                "rounds": self.rounds, "gpu_s": self.gpu_ms / 1e3,
+                "pending": len(self.pending), "active": len(self.active)}
+
+    # ------------------------------------------------------------ internals
+    def _admit(self, now: float):
+        while self.pending:
+            req = self.pending[0]
+            s = self.pool.alloc(req.n)
+            if s < 0:
+                break
+            self.pending.popleft()
+            req.slot0, req.step, req.admitted = s, 0, now
+            self.pose[s:s + req.n].copy_(torch.from_numpy(np.ascontiguousarray(req.poses, np.float32)),
+                                         non_blocking=True)
+            self.state[s:s + req.n].zero_()
+            self.active.append(req)
+
+    def _ligands(self):
+        key = tuple(r.rid for r in self.active)
+        if key != self._ligset_key:
+            self._ligset = LigandSet([r.ligand for r in self.active], device=self.device)
+            self._ligset_key = key
+        return self._ligset
+
+    def round(self, now: float | None = None):
+        """Admit what fits, advance every active request by round_steps, retire finished ones."""
+        now = time.perf_counter() if now is None else now
+        self._admit(now)
+        if not self.active:
+            return
+        # larger ligands first: they take the longest tiles
+        order = sorted(range(len(self.active)), key=lambda i: -len(self.active[i].ligand[0]))
+        segs = [Segment(self.active[i].receptor, i, self.active[i].n, self.active[i].step, self.active[i].slot0)
+                for i in order]
+        wl = Workload(self.grids, self._ligands(), segs, self.launch.lanes_per_pose, self.device,
+                      n_poses=self.capacity)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        minimise(wl, self.pose, self.round_steps, self.adam, self.opts, pose_out=self.pose,
+                 adam_state=self.state, launch=self.launch, scratch=self.scratch)
+        e1.record()
+        e1.synchronize()
+        self.gpu_ms += e0.elapsed_time(e1)
+        self.rounds += 1
+        t = time.perf_counter()
+        still = []
+        for r in self.active:
+            r.step += self.round_steps
+            if r.step >= self.steps:
+                sl = slice(r.slot0, r.slot0 + r.n)
+                r.result_poses = self.pose[sl].cpu().numpy()
+                r.result_energies = self.scratch.energy[sl].cpu().numpy()
+                r.result_status = self.scratch.status[sl].cpu().numpy()
+                r.finished = t
+                self.pool.release(r.slot0, r.n)
+                self.done.append(r)
+            else:
+                still.append(r)
+        self.active = still
+
+
+def replay(server: DockingServer, requests, duration: float | None = None, time_scale: float = 1.0):
+    """Feed requests (dicts with arrival time ``t``) to the server in wall-clock
+    time (``t * time_scale`` after start); returns the server's stats for the
+    requests that arrived within ``duration``."""
+    t0 = time.perf_counter()
+    queue = deque(sorted(requests, key=lambda r: r["t"]))
+    while True:
+        now = time.perf_counter() - t0
+        if duration is not None and now > duration:
+            break
+        while queue and queue[0]["t"] * time_scale <= now:
+            q = queue.popleft()
+            server.submit(Request(q["receptor"], q["ligand"], q["poses"]), now=t0 + q["t"] * time_scale)
+        if server.idle():
+            if not queue:
+                break
+            time.sleep(min(0.001, max(0.0, queue[0]["t"] * time_scale - now)))
+            continue
+        server.round()
+    return server.stats(since=t0)

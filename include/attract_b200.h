@@ -112,6 +112,9 @@ typedef struct AttSegment {
   int lig;      /* ligand index (base index when pose_lig is given) */
   int pose0;    /* first pose of the run */
   int n_poses;
+  int step0;    /* ADAM steps these poses' adam_state has already taken (added to
+                   AttAdamCfg.step0): runs at different stages share one launch */
+  int pad_[3];
 } AttSegment;
 
 typedef struct AttEvalCfg {

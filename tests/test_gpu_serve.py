@@ -1,0 +1,77 @@
+"""Continuous-batching server: a request's result is the same alone and in a
+mix of receptors, ligand sizes and arrival times; rounds equal one launch."""
+import numpy as np
+import pytest
+import torch
+
+from gpu_cases import small_case, to_device_grid
+
+pytestmark = pytest.mark.gpu
+
+
+def _server(grids, **kw):
+    import attract_b200 as A
+    from attract_b200.serve import DockingServer
+
+    A.load_library()
+    return DockingServer(grids, **kw)
+
+
+def _req(seed, receptor, n_beads, n_poses):
+    from attract_b200.serve import Request
+
+    rng = np.random.default_rng(seed)
+    lig = rng.normal(size=(n_beads, 3)) * 1.5
+    lig -= lig.mean(0)
+    t = rng.integers(0, 4, n_beads)
+    poses = small_case(seed=100 + seed, n_poses=n_poses)["poses"].astype(np.float32)
+    return Request(receptor, (lig, t, t), poses)
+
+
+@pytest.fixture(scope="module")
+def grids():
+    return [to_device_grid(small_case(seed=s, n_poses=4)) for s in (40, 41, 42)]
+
+
+def test_result_alone_equals_result_in_the_mix(grids):
+    alone = _server(grids, steps=40, round_steps=10, max_inflight_poses=5000)
+    a = alone.submit(_req(1, 1, 13, 70))
+    alone.run_until_idle()
+    mix = _server(grids, steps=40, round_steps=10, max_inflight_poses=5000)
+    others = [mix.submit(_req(2, 0, 5, 40)), mix.submit(_req(3, 2, 30, 90))]
+    mix.round()                       # the others are on the GPU ...
+    b = mix.submit(_req(1, 1, 13, 70))  # ... when the request arrives
+    mix.submit(_req(4, 1, 22, 33))
+    mix.round()
+    mix.submit(_req(5, 0, 9, 51))
+    mix.run_until_idle()
+    assert b.result_poses is not None and all(o.result_poses is not None for o in others)
+    assert np.array_equal(a.result_poses, b.result_poses)
+    assert np.array_equal(a.result_energies, b.result_energies)
+    st = mix.stats()
+    assert st["requests"] == 5 and st["p99_s"] >= st["p50_s"] > 0
+
+
+def test_rounds_equal_one_launch(grids):
+    import attract_b200 as A
+
+    srv = _server(grids, steps=40, round_steps=10, max_inflight_poses=5000)
+    r = srv.submit(_req(6, 2, 17, 64))
+    srv.run_until_idle()
+    lig = r.ligand
+    wl = A.Workload([grids[2]], A.LigandSet([lig]), [A.Segment(0, 0, 64)], lanes_per_pose=32)
+    out, E, _, _ = A.minimise(wl, torch.tensor(r.poses, device="cuda"), 40, launch=A.LaunchShape(32))
+    assert np.allclose(out.cpu().numpy(), r.result_poses, rtol=1e-5, atol=1e-5)
+    assert np.allclose(E.cpu().numpy(), r.result_energies, rtol=1e-4, atol=1e-4)
+
+
+def test_pool_admission_and_recycling(grids):
+    srv = _server(grids, steps=20, round_steps=10, max_inflight_poses=100)
+    reqs = [srv.submit(_req(10 + i, i % 3, 8, 60)) for i in range(4)]  # 240 poses, pool of 100
+    srv.round()
+    assert len(srv.active) == 1 and len(srv.pending) == 3
+    srv.run_until_idle()
+    assert all(r.result_energies is not None and np.all(np.isfinite(r.result_energies)) for r in reqs)
+    assert srv.pool.used == 0
+    with pytest.raises(ValueError):
+        srv.submit(_req(20, 0, 8, 101))

@@ -211,23 +211,34 @@ class DockingServer:
         self.active = still
 
 
-def replay(server: DockingServer, requests, duration: float | None = None, time_scale: float = 1.0):
-    """Feed requests (dicts with arrival time ``t``) to the server in wall-clock
-    time (``t * time_scale`` after start); returns the server's stats for the
-    requests that arrived within ``duration``."""
+def replay(server: DockingServer, requests, duration: float | None = None, time_scale: float = 1.0,
+           pose_source=None):
+    """Feed requests (dicts with arrival time ``t``, ``receptor``, ``ligand`` and
+    ``poses`` -- or ``n_poses`` drawn from ``pose_source(n)``) to the server in
+    wall-clock time (``t * time_scale`` after start) for ``duration`` seconds.
+    Returns the server's stats for the requests that arrived in the window and
+    finished, plus the number that arrived."""
     t0 = time.perf_counter()
     queue = deque(sorted(requests, key=lambda r: r["t"]))
+    arrived = 0
     while True:
         now = time.perf_counter() - t0
         if duration is not None and now > duration:
             break
         while queue and queue[0]["t"] * time_scale <= now:
             q = queue.popleft()
-            server.submit(Request(q["receptor"], q["ligand"], q["poses"]), now=t0 + q["t"] * time_scale)
+            poses = q["poses"] if "poses" in q else pose_source(q["n_poses"])
+            server.submit(Request(q["receptor"], q["ligand"], poses), now=t0 + q["t"] * time_scale)
+            arrived += 1
         if server.idle():
             if not queue:
                 break
             time.sleep(min(0.001, max(0.0, queue[0]["t"] * time_scale - now)))
             continue
         server.round()
-    return server.stats(since=t0)
+    st = server.stats(since=t0)
+    st["arrived"] = arrived
+    st["window_s"] = time.perf_counter() - t0
+    st["backlog_requests"] = len(server.pending) + len(server.active)
+    st["backlog_poses"] = int(sum(r.n for r in server.pending) + sum(r.n for r in server.active))
+    return st

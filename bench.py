@@ -49,7 +49,11 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--threads", type=int, default=0)
-    ap.add_argument("--cpu-poses", type=int, default=16, help="poses per fragment in the CPU sample")
+    ap.add_argument("--cpu-poses", type=int, default=128, help="poses per fragment in the CPU sample")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other workloads (configs 0, 2, 3)")
+    ap.add_argument("--serve-seconds", type=float, default=20.0,
+                    help="length of the serving run (0 = skip; the full serving workload is 600 s)")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="request arrivals per second")
     return ap.parse_args()
 
 
@@ -195,6 +199,142 @@ def traffic_from_profile(n_launch_units):
     return vals["per"] * n_launch_units
 
 
+# --------------------------------------------------------------------------- other workloads
+def _timed(fn, reps, warm=2):
+    import torch
+
+    for _ in range(warm):
+        fn()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def _peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    return float(json.load(open(p)).get("hbm_gbs", 6650.0)) if os.path.exists(p) else 6650.0
+
+
+def other_configs(args, device, shape):
+    """Plain small (config 0), neighbour-list heavy (config 2) and the
+    differentiation workload (config 3), each on its own synthetic receptor."""
+    import torch
+
+    import attract_b200 as A
+    from attract_b200 import synth
+    from attract_b200.autograd import docking_energy
+    from attract_b200.autotune import autotune
+    from attract_b200.poses import euler_to_Q
+
+    res = {}
+    names = {0: "plain small: 1200-bead receptor, 7-bead fragment, 4096 poses, 1 eval + 100 ADAM steps",
+             2: "nbgrid-heavy: 5000 beads at 0.01/A^3, 40-bead ligand, 500000 surface poses, 1 eval + 50 ADAM"}
+    for idx in (0, 2):
+        cfg = synth.make_config(idx, seed=0, scale=args.scale)
+        grid = A.Grid.build(cfg.rec_xyz, cfg.rec_type, cfg.ff, cfg.geom, cutoff=cfg.cutoff, device=device)
+        ligs = A.LigandSet(cfg.ligands, device=device)
+        poses_np = np.concatenate(cfg.poses).astype(np.float32)
+        poses = torch.tensor(poses_np, device=device)
+        wl = A.Workload([grid], ligs, [A.Segment(0, i, len(p)) for i, p in enumerate(cfg.poses)])
+        shp, _ = autotune(wl, poses, use_cache=False)
+        wl = wl.with_lanes(shp.lanes_per_pose)
+        _, _, _, st = A.minimise(wl, poses, cfg.steps, launch=shp, stats=True)
+        stats = st.cpu().numpy()
+        scratch = A.MinimiseScratch(wl.n_poses, device)
+        out = torch.empty_like(poses)
+        ms = _timed(lambda: A.minimise(wl, poses, cfg.steps, launch=shp, pose_out=out, scratch=scratch), 5)
+        e = {"workload": names[idx], "poses": wl.n_poses, "adam_steps": cfg.steps, "value": round(wl.n_poses / ms * 1e3, 1),
+             "unit": UNIT, "ms": round(ms, 3), "launch": {"lanes_per_pose": shp.lanes_per_pose},
+             "roofline_frac": round(algorithmic_bytes(stats) / (ms / 1e3) / 1e9 / _peak(), 4),
+             "list_entries_per_lookup": round(float(stats[2]) / max(float(stats[1]), 1.0), 2)}
+        if idx == 2:
+            # list lengths seen by the starting poses' beads (the workload's "0-80 entries")
+            xyz = np.asarray(cfg.ligands[0][0])
+            X = np.einsum("bij,nj->bni", euler_to_Q(*poses_np[:20000, :3].T), xyz) + poses_np[:20000, None, 3:]
+            g = cfg.geom
+            v = (X - np.asarray(g.origin)) / g.spacing
+            inn = np.all((v >= 0) & (v < np.asarray(g.dim) - 1), axis=2)
+            near = np.floor(v + 0.5).astype(np.int64)
+            hdr = grid.nb_hdr.cpu().numpy().view(np.uint32)
+            vox = (near[..., 0] * g.dim[1] + near[..., 1]) * g.dim[2] + near[..., 2]
+            cnt = np.where(inn, hdr[np.clip(vox, 0, len(hdr) - 1), 1], 0)
+            e["bead_fraction_with_lists"] = round(float((cnt > 0).mean()), 3)
+            e["list_length_hist"] = np.bincount(np.minimum(cnt[cnt > 0], 80), minlength=81).tolist()
+            e["list_length_max"] = int(cnt.max())
+        res[f"config{idx}"] = e
+        del grid, wl, scratch
+        torch.cuda.empty_cache()
+    cfg = synth.make_config(3, seed=0, scale=args.scale)
+    grid = A.Grid.build(cfg.rec_xyz, cfg.rec_type, cfg.ff, cfg.geom, cutoff=cfg.cutoff, keep_dense=True,
+                        device=device)
+    grid.inner.requires_grad_(True)
+    grid.outer.requires_grad_(True)
+    wl = A.Workload([grid], A.LigandSet(cfg.ligands, device=device), [A.Segment(0, 0, len(cfg.poses[0]))],
+                    lanes_per_pose=32)
+    P = torch.tensor(cfg.poses[0].astype(np.float32), device=device, requires_grad=True)
+
+    def fwd_bwd():
+        P.grad = None
+        grid.inner.grad = None
+        grid.outer.grad = None
+        docking_energy(wl, P, A.EvalOptions(grad_mode="analytic")).backward()
+
+    ms = _timed(fwd_bwd, 10)
+    res["config3"] = {"workload": "differentiation: config-1 receptor, 24-bead ligand, 65536 poses, summed energy, "
+                                  "backward to poses and grid energies (analytic mode)",
+                      "poses": wl.n_poses, "ms_forward_backward": round(ms, 3),
+                      "value": round(wl.n_poses / ms * 1e3, 1), "unit": "poses/s (forward+backward)"}
+    del grid, wl
+    torch.cuda.empty_cache()
+    return res
+
+
+def serving_run(args, device):
+    """Four resident receptors, Poisson arrivals, lognormal pose counts,
+    continuous batching in rounds of 25 ADAM steps (200 per request).  Run
+    at the workload's arrival rate and, when that overloads the GPU, again at
+    60% of the throughput it sustained, where p50/p99 describe a stable queue."""
+    import torch
+
+    import attract_b200 as A
+    from attract_b200 import synth
+    from attract_b200.poses import random_in_ball, random_rotations
+    from attract_b200.serve import DockingServer, replay
+
+    ff, recs = synth.serving_mix(seed=0)
+    grids = [A.Grid.build(xyz, t, ff, geom, device=device) for xyz, t, R, geom in recs]
+    rng = np.random.default_rng(1)
+    pool = np.concatenate([random_rotations(400_000, rng), random_in_ball(400_000, 30.0, rng)], 1).astype(np.float32)
+    draw = lambda n: pool[(o := int(rng.integers(0, len(pool) - n))):o + n]
+    desc = ("4 resident receptors (1500/3000/4500/6000 beads), ligands U{5..60} beads, poses lognormal(median "
+            "10000, sigma 1.0) clipped to [1000, 200000], 200 ADAM steps in rounds of 25")
+
+    def one(rate):
+        srv = DockingServer(grids, steps=200, round_steps=25, max_inflight_poses=600_000, hbm_budget_bytes=150e9,
+                            launch=A.LaunchShape(32))
+        reqs = synth.serving_requests(int(args.serve_seconds * rate * 1.5) + 10, seed=0, rate=rate)
+        st = replay(srv, reqs, duration=args.serve_seconds, pose_source=draw)
+        offered = sum(q["n_poses"] for q in reqs if q["t"] <= args.serve_seconds) / args.serve_seconds
+        st.update({"arrival_rate_per_s": rate, "offered_poses_per_s": round(offered, 1),
+                   "mean_poses_per_request": round(float(np.mean([q["n_poses"] for q in reqs])), 1),
+                   "resident_grid_gb": round(srv.grid_bytes / 1e9, 2), "pool_poses": srv.capacity})
+        del srv
+        return st
+
+    out = {"workload": desc, "window_s_requested": args.serve_seconds, "runs": [one(args.serve_rate)]}
+    first = out["runs"][0]
+    if first["backlog_requests"] > 0 and first["poses_per_s"]:
+        out["runs"].append(one(round(0.6 * first["poses_per_s"] / first["mean_poses_per_request"], 1)))
+    del grids
+    torch.cuda.empty_cache()
+    return out
+
+
 # --------------------------------------------------------------------------- ours
 def run_ours(args):
     import torch
@@ -332,6 +472,13 @@ def run_ours(args):
         out["batched_vs_plain"] = round(out["value"] / out["plain"]["value"], 2)
     if not args.no_cpu and rank == 0 and world == 1:
         out["cpu_baseline"] = cpu_baseline(cfg, grid, order, args.cpu_poses, steps)
+    if rank == 0 and world == 1 and (not args.no_configs or args.serve_seconds > 0):
+        del plan, grid, wl
+        torch.cuda.empty_cache()
+        if not args.no_configs:
+            out["configs"] = other_configs(args, device, shape)
+        if args.serve_seconds > 0:
+            out["serving"] = serving_run(args, device)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -3,27 +3,26 @@
 // A pose is served by a team of S lanes (S = 8, 16 or 32: 32/S poses per warp).
 // Team lane l owns ligand beads l, l+S, ... (K beads per lane, N <= K*S); the
 // ligand-frame coordinates stay in registers for the whole minimisation.  One
-// evaluation of a pose runs in four phases:
+// evaluation of a pose runs in three phases:
 //
-//  A  every owner lane moves its beads, computes the voxel, and starts a
-//     128-byte bulk copy (TMA engine, cp.async.bulk) of the bead's grid brick --
-//     the 8 trilinear corners of the voxel, (E, Fx, Fy, Fz) each -- into its
-//     shared-memory slot, completing on the warp's mbarrier; it also loads the
-//     bead's neighbour-list header {start, count};
-//  B  a team scan of the list lengths gives every bead's offset in the team's
-//     flattened list of (bead, entry) pairs;
-//  C  the team walks that flattened list, each lane a contiguous chunk, with all
-//     list-entry loads of a chunk issued before the receptor loads and the pair
-//     math -- so the bricks stream in while the pair terms are computed;
-//  D  after the mbarrier completes, each owner reads its brick from shared
-//     memory (rotated chunk order: conflict-free) and adds the grid term.
+//  A  every owner lane moves its beads, computes the voxel, and copies the
+//     bead's 128-byte grid brick -- the 8 trilinear corners of the voxel,
+//     (E, Fx, Fy, Fz) each -- and the fixed-size neighbour record of its
+//     nearest inner grid point into the warp's shared memory with 16-byte
+//     asynchronous copies (cp.async: one warp instruction moves a piece for
+//     every lane), then waits for its own copies;
+//  C  neighbour pairs: the owners write their beads' list entries into the
+//     team's pair buffer, and the team's lanes take the pairs round-robin
+//     (balanced whatever the per-bead list lengths);
+//  D  each owner interpolates its brick from shared memory (rotated corner
+//     order: conflict-free) and adds the grid term.
 //
 // Energy, dE/dt and the torque are linear in every corner / pair contribution,
 // so each lane accumulates its own share and the team sums 7 values with
 // xor-shuffles per evaluation.  The rigid-body ADAM step runs on team lanes
 // 0..5 between evaluations; a persistent launch pulls tiles of poses from a
-// work counter.  Every mbarrier wait is bounded; a timeout sets an error word
-// and the warp returns.
+// work counter.  The kernels hold no spin-wait: every wait is on the issuing
+// thread's own copies or a warp barrier.
 //
 // Semantics follow test5.py (sjdv1982/attract-jax):
 //   transform            [x,1] @ mat                    test5.py:315-317
@@ -71,17 +70,23 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// 128-byte brick: global -> shared through the bulk-copy (TMA) engine
-// (bytes: a multiple of 16; both addresses 16-B aligned)
+// global -> shared through the bulk-copy (TMA) engine, completing on `bar`
+// (bytes: a multiple of 16; both addresses 16-B aligned).  A 128-B brick is
+// one line: the engine moves it without L1 wavefronts, unlike 16-B per-lane
+// copies, which saturate L1TEX on this gather.
 __device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
 
+// orders this thread's generic-proxy shared-memory reads before later
+// async-proxy (bulk-copy) writes to the same bytes
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+
+constexpr int WAIT_LIMIT = 1 << 22;  // try_wait polls before a bulk-copy wait is declared hung
 
 // Loads with a fixed state space.  A list entry comes either from the
 // shared-memory record or from global memory; written as two distinct
@@ -109,8 +114,6 @@ struct __align__(16) BeadArm {  // lever arm for the torque (Q x) or ligand-fram
   float x, y, z, pad;
 };
 
-constexpr int WAIT_LIMIT = 1 << 22;  // try_wait polls before a bulk-copy wait is declared hung
-
 // device-wide error word of the scoring kernels (ATT_KERR_* bits), read and
 // cleared by att_kernel_status()
 __device__ int g_kernel_error = 0;
@@ -133,10 +136,15 @@ __device__ __noinline__ void bounds_report(int code, long long a, long long b) {
 #endif
 
 // shared memory of one warp: per bead slot a 128-B brick, a neighbour-record
-// slot of rec_slot bytes and two 16-B bead records, then the mbarrier
+// slot of rec_slot bytes and two 16-B bead records; the pair buffers of the
+// warp's teams (PAIRS_PER_BEAD u32 words per bead slot, plus S words of
+// padding per team so that teams start in different banks); the mbarrier
+constexpr int PAIRS_PER_BEAD = 8;
 __host__ __device__ inline int rec_stride(int rec_slot) { return rec_slot ? rec_slot + 16 : 0; }
+__host__ __device__ inline size_t pair_buffer_bytes(int K) { return (size_t)32 * (PAIRS_PER_BEAD * K + 1) * 4; }
 __host__ __device__ inline size_t warp_smem_bytes(int K, int rec_slot) {
-  return (size_t)32 * K * (128 + rec_stride(rec_slot) + sizeof(BeadPos) + sizeof(BeadArm)) + 16;
+  return (size_t)32 * K * (128 + rec_stride(rec_slot) + sizeof(BeadPos) + sizeof(BeadArm)) + pair_buffer_bytes(K) +
+         16;
 }
 
 template <int S>
@@ -191,7 +199,8 @@ template <int S, int K, int MODE>
 __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kernel(const __grid_constant__ KParams p) {
   constexpr int P = 32 / S;      // poses per warp
   constexpr int NB = S * K;      // bead slots per pose
-  constexpr int U = 4;           // list entries in flight per lane
+  constexpr int U = 2;           // pair slots in flight per lane
+  constexpr int PB = PAIRS_PER_BEAD * NB;  // pair-buffer window of one team
   constexpr bool MAT = (MODE == MODE_EVAL_MAT);
   extern __shared__ __align__(128) unsigned char smem_raw[];
 
@@ -206,8 +215,10 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
   unsigned char* nrec = wsm + 32 * K * 128;                                 // [32K][RS]
   BeadPos* bpos = reinterpret_cast<BeadPos*>(nrec + 32 * K * RS);
   BeadArm* barm = reinterpret_cast<BeadArm*>(nrec + 32 * K * (RS + 16));
-  uint64_t* bar = reinterpret_cast<uint64_t*>(nrec + 32 * K * (RS + 32));
+  uint32_t* pbuf = reinterpret_cast<uint32_t*>(nrec + 32 * K * (RS + 32));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(nrec + 32 * K * (RS + 32) + pair_buffer_bytes(K));
   const int tbase = slot * NB;  // this team's first bead record
+  uint32_t* pb = pbuf + slot * (PB + S);  // this team's pair buffer
 
   // Grid descriptors: copied from the parameters into shared memory with static
   // parameter offsets only, so that the per-segment grid is picked by a
@@ -225,7 +236,9 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
   __syncwarp();
   uint32_t parity = 0;
 
-  unsigned c_grid = 0, c_look = 0, c_ent = 0;  // statistics (MODE_MIN)
+  // statistics (MODE_MIN): bead evaluations with a brick, list lookups, list
+  // entries, brick copies, record copies
+  unsigned c_grid = 0, c_look = 0, c_ent = 0, c_cpb = 0, c_cpr = 0;
 
   int tile;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -249,7 +262,8 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
     const int loff = __ldg(p.lig_off + lig);
     const int Ntot = valid ? __ldg(p.lig_off + lig + 1) - loff : 0;
     // ligands larger than the team's NB bead slots are evaluated in chunks of
-    // NB beads; the chunk count is warp-uniform (the mbarrier is per warp)
+    // NB beads; the chunk count is warp-uniform (the chunk loop holds warp
+    // barriers and shuffles)
     const int nchunk = __reduce_max_sync(0xffffffffu, (unsigned)((Ntot + NB - 1) / NB));
     const bool multi = nchunk > 1;
 
@@ -271,6 +285,12 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
       }
     };
     load_beads(0);
+    // what this lane's shared-memory slots hold: brick index and record grid
+    // point per owned bead (-1: nothing valid).  A bead moves ~0.1 A per ADAM
+    // step against 0.9 A cells, so most steps find both still in place.
+    int held_b[K], held_v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) held_b[k] = held_v[k] = -1;
 
     // pose state: team lane k < 6 owns DOF k
     float my_x = 0.f, my_m = 0.f, my_v = 0.f;
@@ -414,29 +434,45 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
           barm[tbase + i] = ba;
         }
       }
-      // one bulk copy per brick and per neighbour record; the mbarrier phase
-      // completes when lane 0 has arrived and all bytes have landed (copies
-      // may finish before the arrive)
+      // One bulk copy per brick and per neighbour record whose slot does not
+      // already hold it (chunked ligands share the slots: always copy).  The
+      // mbarrier phase completes when lane 0 has arrived and all bytes have
+      // landed (copies may finish before the arrive); a warp whose slots are
+      // all current skips the copy round.
+      if (multi) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) held_b[k] = held_v[k] = -1;
+      }
+      bool need_b[K], need_v[K];
       unsigned my_bytes = 0;
 #pragma unroll
-      for (int k = 0; k < K; ++k)
-        my_bytes += (use[k] ? 128u : 0u) + (nvox[k] >= 0 ? (unsigned)G.nb_rec_bytes : 0u);
-      const unsigned warp_bytes = __reduce_add_sync(0xffffffffu, my_bytes);
-      if (lane == 0) mbar_arrive_expect_tx(bar, warp_bytes);
-      __syncwarp();
-#pragma unroll
       for (int k = 0; k < K; ++k) {
-        const int sk = tbase + tl + k * S;
-        if (use[k]) {
-          bulk_copy(bricks + (size_t)sk * 8, G.bricks + bidx[k] * 8, 128u, bar);
-          if (MODE == MODE_MIN) c_grid += 1;
-        }
-        if (nvox[k] >= 0) {
-          bulk_copy(nrec + (size_t)sk * RS, G.nb_rec + nvox[k] * G.nb_rec_bytes, (unsigned)G.nb_rec_bytes, bar);
-          if (MODE == MODE_MIN) c_look += 1;
+        need_b[k] = use[k] && (int)bidx[k] != held_b[k];
+        need_v[k] = nvox[k] >= 0 && (int)nvox[k] != held_v[k];
+        my_bytes += (need_b[k] ? 128u : 0u) + (need_v[k] ? (unsigned)G.nb_rec_bytes : 0u);
+        if (MODE == MODE_MIN) {
+          c_grid += use[k] ? 1u : 0u;
+          c_look += nvox[k] >= 0 ? 1u : 0u;
+          c_cpb += need_b[k] ? 1u : 0u;
+          c_cpr += need_v[k] ? 1u : 0u;
         }
       }
-      {
+      const unsigned warp_bytes = __reduce_add_sync(0xffffffffu, my_bytes);
+      if (warp_bytes != 0) {
+        if (lane == 0) mbar_arrive_expect_tx(bar, warp_bytes);
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const int sk = tbase + tl + k * S;
+          if (need_b[k]) {
+            bulk_copy(bricks + (size_t)sk * 8, G.bricks + bidx[k] * 8, 128u, bar);
+            held_b[k] = (int)bidx[k];
+          }
+          if (need_v[k]) {
+            bulk_copy(nrec + (size_t)sk * RS, G.nb_rec + nvox[k] * G.nb_rec_bytes, (unsigned)G.nb_rec_bytes, bar);
+            held_v[k] = (int)nvox[k];
+          }
+        }
         bool done = false;
         for (int it = 0; it < WAIT_LIMIT && !done; ++it) done = mbar_try_wait(bar, parity);
         if (!__all_sync(0xffffffffu, done)) {
@@ -446,77 +482,98 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
         parity ^= 1u;
       }
 
-      // ---------------- phase C: neighbour lists, bead-major: each owner lane
-      // walks its own beads' lists (inline entries from the shared-memory
-      // record, the rest from the CSR overflow) with the bead in registers,
-      // U entries in flight, and one torque cross product per bead
-      const unsigned ninl = (unsigned)G.nb_inline;
+      // ---------------- phase C: neighbour pairs, balanced over the team.
+      // C1: every owner lane writes its beads' list entries (inline ones from
+      // the shared-memory record, the rest from the CSR overflow) as
+      // (receptor bead | bead slot << 16) words into the team's pair buffer,
+      // runs in lane order.  C2: the team's lanes take the buffered pairs
+      // round-robin, U in flight, and add energy, force and torque per pair.
+      // Teams with more pairs than the buffer holds take several windows.
+      {
+        const unsigned ninl = (unsigned)G.nb_inline;
+        unsigned ck[K];
+        unsigned my_total = 0;
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const int i = tl + k * S;
-        const unsigned char* rk = nrec + (size_t)(tbase + i) * RS;
-        const unsigned cnt = (nvox[k] >= 0) ? *reinterpret_cast<const uint16_t*>(rk + 4) : 0u;
-        if (MODE == MODE_MIN) c_ent += cnt;
-        if (cnt == 0) continue;
-        const unsigned ovf = *reinterpret_cast<const unsigned*>(rk);
-#ifdef ATT_BOUNDS_CHECK
-        if (cnt > ninl && !ATT_CHECK((long long)ovf - ninl + cnt <= G.n_list, 6, ovf, cnt)) continue;
-#endif
-        const uint16_t* inl = reinterpret_cast<const uint16_t*>(rk + 6);
-        const BeadPos bp = bpos[tbase + i];
-        float ge = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-        for (unsigned li = 0; li < cnt; li += U) {
-          unsigned jj[U];
-#pragma unroll
-          for (int m = 0; m < U; ++m) {
-            const unsigned idx = li + m;
-#ifdef ATT_BOUNDS_CHECK
-            unsigned j = ATT_NB_EMPTY;
-            if (idx < cnt) {
-              if (idx < ninl) {
-                j = lds_u16(inl + idx);
-              } else {
-                const long long oi = (long long)ovf + (long long)(idx - ninl);
-                if (ATT_CHECK(oi >= 0 && oi < G.n_list, 3, oi, G.n_list)) j = ldg_u16(G.nb_list + oi);
-              }
-              if (j != ATT_NB_EMPTY && !ATT_CHECK(j < (unsigned)G.n_rec, 4, j, G.n_rec)) j = ATT_NB_EMPTY;
-            }
-            jj[m] = j;
-#else
-            unsigned j = ATT_NB_EMPTY;
-            if (idx < cnt) {
-              if (idx < ninl) j = lds_u16(inl + idx);
-              else j = ldg_nc_u16(G.nb_list + (ovf + (idx - ninl)));
-            }
-            jj[m] = j;
-#endif
-          }
-          float4 rr[U];
-#pragma unroll
-          for (int m = 0; m < U; ++m)
-            rr[m] = (jj[m] < (unsigned)G.n_rec) ? ldg_f4(G.rec + jj[m]) : make_float4(1e15f, 1e15f, 1e15f, 0.f);
-#pragma unroll
-          for (int m = 0; m < U; ++m) {
-            float px, py, pz;
-            pair_term_masked(p, G, bp, rr[m], ge, px, py, pz);
-            gx += px;
-            gy += py;
-            gz += pz;
-          }
+        for (int k = 0; k < K; ++k) {
+          const unsigned char* rk = nrec + (size_t)(tbase + tl + k * S) * RS;
+          ck[k] = (nvox[k] >= 0) ? lds_u16(rk + 4) : 0u;
+          my_total += ck[k];
         }
-        const BeadArm ba = barm[tbase + i];
-        acc_e += ge;
-        acc_gx += gx;
-        acc_gy += gy;
-        acc_gz += gz;
-        if (MAT) {
-          acc_t[0] = fmaf(ba.x, gx, acc_t[0]); acc_t[1] = fmaf(ba.x, gy, acc_t[1]); acc_t[2] = fmaf(ba.x, gz, acc_t[2]);
-          acc_t[3] = fmaf(ba.y, gx, acc_t[3]); acc_t[4] = fmaf(ba.y, gy, acc_t[4]); acc_t[5] = fmaf(ba.y, gz, acc_t[5]);
-          acc_t[6] = fmaf(ba.z, gx, acc_t[6]); acc_t[7] = fmaf(ba.z, gy, acc_t[7]); acc_t[8] = fmaf(ba.z, gz, acc_t[8]);
-        } else {
-          acc_t[0] = fmaf(ba.y, gz, fmaf(-ba.z, gy, acc_t[0]));
-          acc_t[1] = fmaf(ba.z, gx, fmaf(-ba.x, gz, acc_t[1]));
-          acc_t[2] = fmaf(ba.x, gy, fmaf(-ba.y, gx, acc_t[2]));
+        if (MODE == MODE_MIN) c_ent += my_total;
+        unsigned incl = my_total;  // inclusive scan over the team's lanes
+#pragma unroll
+        for (int off = 1; off < S; off <<= 1) {
+          const unsigned v = __shfl_up_sync(0xffffffffu, incl, off, S);
+          if (tl >= off) incl += v;
+        }
+        const unsigned team_total = __shfl_sync(0xffffffffu, incl, S - 1, S);
+        const unsigned run0 = incl - my_total;  // buffer position of this lane's first entry
+        const unsigned warp_max = __reduce_max_sync(0xffffffffu, team_total);
+        for (unsigned q0 = 0; q0 < warp_max; q0 += PB) {
+          unsigned r = run0;
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const unsigned lo = max(q0, r), hi = min(r + ck[k], q0 + PB);
+            if (lo < hi) {
+              const unsigned char* rk = nrec + (size_t)(tbase + tl + k * S) * RS;
+              const unsigned ovf = *reinterpret_cast<const unsigned*>(rk);
+              const uint16_t* inl = reinterpret_cast<const uint16_t*>(rk + 6);
+              const unsigned tag = (unsigned)(tl + k * S) << 16;
+#ifdef ATT_BOUNDS_CHECK
+              if (ck[k] > ninl && !ATT_CHECK((long long)ovf - ninl + ck[k] <= G.n_list, 6, ovf, ck[k])) {
+                for (unsigned s = lo; s < hi; ++s) pb[s - q0] = ATT_NB_EMPTY | tag;
+                r += ck[k];
+                continue;
+              }
+#endif
+              for (unsigned s = lo; s < hi; ++s) {
+                const unsigned e = s - r;
+                const unsigned j = (e < ninl) ? lds_u16(inl + e) : ldg_nc_u16(G.nb_list + (ovf + (e - ninl)));
+                pb[s - q0] = j | tag;
+              }
+            }
+            r += ck[k];
+          }
+          __syncwarp();
+          const unsigned n = min(team_total - min(team_total, q0), (unsigned)PB);
+          for (unsigned s0 = tl; s0 < n; s0 += U * S) {
+            unsigned ww[U];
+#pragma unroll
+            for (int m = 0; m < U; ++m) {
+              const unsigned s = s0 + m * S;
+              ww[m] = (s < n) ? pb[s] : (unsigned)ATT_NB_EMPTY;
+            }
+            float4 rr[U];
+#pragma unroll
+            for (int m = 0; m < U; ++m) {
+              const unsigned j = ww[m] & 0xffffu;
+#ifdef ATT_BOUNDS_CHECK
+              if (j != ATT_NB_EMPTY) (void)ATT_CHECK(j < (unsigned)G.n_rec, 4, j, G.n_rec);
+#endif
+              rr[m] = (j < (unsigned)G.n_rec) ? ldg_f4(G.rec + j) : make_float4(1e15f, 1e15f, 1e15f, 0.f);
+            }
+#pragma unroll
+            for (int m = 0; m < U; ++m) {
+              const unsigned bi = tbase + (ww[m] >> 16);
+              const BeadPos bp = bpos[bi];
+              float px, py, pz;
+              pair_term_masked(p, G, bp, rr[m], acc_e, px, py, pz);
+              const BeadArm ba = barm[bi];
+              acc_gx += px;
+              acc_gy += py;
+              acc_gz += pz;
+              if (MAT) {
+                acc_t[0] = fmaf(ba.x, px, acc_t[0]); acc_t[1] = fmaf(ba.x, py, acc_t[1]); acc_t[2] = fmaf(ba.x, pz, acc_t[2]);
+                acc_t[3] = fmaf(ba.y, px, acc_t[3]); acc_t[4] = fmaf(ba.y, py, acc_t[4]); acc_t[5] = fmaf(ba.y, pz, acc_t[5]);
+                acc_t[6] = fmaf(ba.z, px, acc_t[6]); acc_t[7] = fmaf(ba.z, py, acc_t[7]); acc_t[8] = fmaf(ba.z, pz, acc_t[8]);
+              } else {
+                acc_t[0] = fmaf(ba.y, pz, fmaf(-ba.z, py, acc_t[0]));
+                acc_t[1] = fmaf(ba.z, px, fmaf(-ba.x, pz, acc_t[1]));
+                acc_t[2] = fmaf(ba.x, py, fmaf(-ba.y, px, acc_t[2]));
+              }
+            }
+          }
+          __syncwarp();  // the next window overwrites the buffer
         }
       }
 
@@ -671,9 +728,9 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
   }
 
   if (MODE == MODE_MIN && p.stats != nullptr) {
-    unsigned long long v[3] = {c_grid, c_look, c_ent};
+    unsigned long long v[5] = {c_grid, c_look, c_ent, c_cpb, c_cpr};
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 5; ++k) {
 #pragma unroll
       for (int off = 16; off >= 1; off >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
       if (lane == 0 && v[k]) atomicAdd(p.stats + k, v[k]);

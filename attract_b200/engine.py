@@ -225,7 +225,7 @@ def minimise(wl: Workload, poses: torch.Tensor, steps: int, adam: AdamOptions | 
         _check_pose_lig(wl, pose_lig)
     if scratch is None:
         scratch = MinimiseScratch(B, wl.device)
-    st = torch.zeros(3, dtype=torch.int64, device=wl.device) if stats else None
+    st = torch.zeros(5, dtype=torch.int64, device=wl.device) if stats else None
     cfg = adam.to_c(opts)
     lc = launch.to_c()
     rc = _lib.load().att_minimise(wl.c_grids, len(wl.grids), C.byref(wl.c_ligs), _lib.ptr(wl.segs),

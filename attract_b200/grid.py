@@ -135,7 +135,7 @@ class Grid:
         self._att = None
 
     def _pack_records(self, rec_bytes: int | None = None):
-        """Fixed-size neighbour records (one bulk copy per bead and step): the
+        """Fixed-size neighbour records (copied with the brick per bead and step): the
         smallest of 32/64/128 bytes whose inline entries hold 99 % of the
         non-empty lists; longer lists continue in the CSR list."""
         counts = self.nb_hdr[:, 1]

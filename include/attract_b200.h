@@ -53,7 +53,8 @@ extern "C" {
 #define ATT_STATUS_NONFINITE_ENERGY 2 /* the returned energy is not finite */
 
 /* device-wide kernel error word (att_kernel_status) */
-#define ATT_KERR_COPY_TIMEOUT 1 /* a warp gave up waiting for its grid-brick bulk copies and returned */
+#define ATT_KERR_COPY_TIMEOUT 1 /* reserved: a warp gave up waiting for its copies (the current kernels
+                                   wait only on their own asynchronous copies and never set it) */
 #define ATT_KERR_BOUNDS 2       /* (ATT_BOUNDS_CHECK builds) an index failed its check; the access was skipped */
 
 /* A pose is served by lanes_per_pose lanes holding up to 8 beads each; a
@@ -165,7 +166,9 @@ int att_energrad(const AttGrid* grids, int n_grids, const AttLigands* ligs,
    final evaluation whose energy is returned.  pose_in_dev/pose_out_dev [B][6] (may
    alias); adam_state_dev [B][12] (m[6], v[6]) in/out or NULL (start from zero);
    work_counter_dev: one int of scratch, zeroed by this call; stats_dev: optional
-   [3] u64 counters (bead evaluations, neighbour lookups, list entries visited).
+   [5] u64 counters, added to (bead evaluations with a grid brick, neighbour
+   lookups, list entries visited, brick copies, record copies; a bead copies its
+   brick or record only when it differs from the one its slot holds).
    seg_tile_dev [n_segs+1]: first work tile of each segment (a tile is
    32/lanes_per_pose consecutive poses of one segment).  test5.py:436-467. */
 int att_minimise(const AttGrid* grids, int n_grids, const AttLigands* ligs,
@@ -211,7 +214,8 @@ int att_nbgrid_fill(const AttGridGeom* geom, const float* rec_dev, int n_rec, fl
 /* Fixed-size neighbour records from the CSR lists: record v holds
    {overflow index = start + inline, count, first `inline` entries (rest
    ATT_NB_EMPTY)}; entries beyond the inline ones stay in the CSR list, which
-   the kernels keep reading.  One record is one bulk copy per bead and step.
+   the kernels keep reading.  A bead copies its record into shared memory
+   with the same asynchronous copies as its grid brick, every step.
    records_dev: n_voxels * rec_bytes bytes, 16-B aligned; rec_bytes 32/64/128.
    (No counterpart in the reference: a layout of the neighbour grid of
    read_grid2.py:113-124 for the B200 kernels.) */

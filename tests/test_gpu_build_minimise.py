@@ -181,6 +181,9 @@ def test_minimise_stats_counts():
     assert 0 < st[0] <= 4 * 32 * n_lig
     assert 0 < st[1] <= 4 * 32 * n_lig
     assert st[2] >= 0
+    # copies only when a slot's brick / record changed: at least one per pose
+    # and bead with data, at most one per evaluation
+    assert 0 < st[3] <= st[0] and 0 < st[4] <= st[1]
 
 
 def test_large_ligands_and_chunking():
@@ -214,7 +217,7 @@ def test_large_ligands_and_chunking():
 
 
 def test_zz_kernel_error_word_is_clear():
-    """No warp of any kernel above gave up on a bulk copy."""
+    """No kernel above set the device error word."""
     from attract_b200 import _lib
 
     torch.cuda.synchronize()

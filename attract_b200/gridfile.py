@@ -76,9 +76,19 @@ def _parse(grid_data: bytes, read_gradients: bool):
 
     def array(dtype, count):
         nonlocal pos
+        if count < 0 or pos + np.dtype(dtype).itemsize * count > len(buf):
+            raise GridFileError("truncated grid")
         a = np.frombuffer(buf, dtype=dtype, count=count, offset=pos)
         pos += a.nbytes
         return a
+
+    def long():
+        nonlocal pos
+        if pos + 8 > len(buf):
+            raise GridFileError("truncated grid")
+        (v,) = struct.unpack_from("=q", buf, pos)
+        pos += 8
+        return v
 
     n_eg, shm = ints(2)
     energrads = np.zeros((0, 4), np.float32)
@@ -90,16 +100,14 @@ def _parse(grid_data: bytes, read_gradients: bool):
     if shm != -1:
         raise GridFileError("grid refers to shared memory")
     neighbours = array(_NB_DTYPE, n_nb)["index"]
-    (inner_size,) = struct.unpack_from("=q", buf, pos)
-    pos += 8
+    inner_size = long()
     dx, dy, dz = (int(v) for v in d["dim"])
     if inner_size != dx * dy * dz:
         raise GridFileError(f"inner grid size {inner_size} != {dx}*{dy}*{dz}")
     inner = array(_INNER_DTYPE, inner_size)
     if len(neighbours) and neighbours.max() >= 2 ** 16:
         raise GridFileError("too many atoms for uint16 neighbour lists")
-    (big_size,) = struct.unpack_from("=q", buf, pos)
-    pos += 8
+    big_size = long()
     big = None
     if n_eg:
         dx2, dy2, dz2 = (int(v) for v in d["dim2"])
@@ -168,10 +176,10 @@ def read_grid(grid_data: bytes, read_gradients: bool = False):
     ng[rows, np.arange(len(nb_list)) - np.repeat(off, cnt)] = nb_list
     d["neighbour_grid"] = ng.reshape(dx, dy, dz, maxnb)
     d["max_nr_neighbours"] = d["nr_neighbours"].max()
-    vals = [d.get(f) for f in GRID_FIELDS[:-1]] + [None]
-    keys = [f for f in GRID_FIELDS[:-1] if f in d] + ["neighbour_grid_ravel"]
-    cls = GridTuple if len(keys) == len(GRID_FIELDS) else namedtuple("Grid", keys)
-    return cls(*[d[k] for k in keys[:-1]], None) if cls is not GridTuple else cls(*vals)
+    # a grid without potentials has no inner/outer fields (read_grid2.py:159)
+    keys = [f for f in GRID_FIELDS[:-1] if f in d]
+    cls = GridTuple if len(keys) == len(GRID_FIELDS) - 1 else namedtuple("Grid", keys + ["neighbour_grid_ravel"])
+    return cls(*[d[k] for k in keys], None)
 
 
 def write_grid(*, gridspacing, gridextension, plateaudis, neighbourdis, alphabet, origin, dim, dim2, natoms,
@@ -246,7 +254,7 @@ def write_grid(*, gridspacing, gridextension, plateaudis, neighbourdis, alphabet
     parts.append(struct.pack("=2i", len(nb), -1))
     parts.append(nb.tobytes())
     inner = np.zeros(V, _INNER_DTYPE)
-    inner["potential"] = pot_inner.reshape(dx, dy, dz, 100).transpose(2, 1, 0, 3).reshape(V, 100)
+    inner["potential"] = pot_inner  # rows already in file point order
     inner["neighbourlist"] = np.where(cnt_f > 0, np.cumsum(cnt_f) - cnt_f + 1, 0)
     nr = to_file(np.asarray(nr_neighbours, np.int64).reshape(-1)) if nr_neighbours is not None else cnt_f
     inner["nr_neighbours"] = nr.astype(np.int16)

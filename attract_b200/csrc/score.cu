@@ -5,12 +5,13 @@
 // ligand-frame coordinates stay in registers for the whole minimisation.  One
 // evaluation of a pose runs in three phases:
 //
-//  A  every owner lane moves its beads, computes the voxel, and copies the
-//     bead's 128-byte grid brick -- the 8 trilinear corners of the voxel,
-//     (E, Fx, Fy, Fz) each -- and the fixed-size neighbour record of its
-//     nearest inner grid point into the warp's shared memory with 16-byte
-//     asynchronous copies (cp.async: one warp instruction moves a piece for
-//     every lane), then waits for its own copies;
+//  A  every owner lane moves its beads, computes the voxel, and -- when its
+//     shared-memory slot does not already hold them -- bulk-copies (TMA
+//     engine) the bead's 128-byte grid brick (the 8 trilinear corners of the
+//     voxel, (E, Fx, Fy, Fz) each) and the fixed-size neighbour record of its
+//     nearest inner grid point into the warp's shared memory, completing on
+//     the warp's mbarrier.  A bead moves ~0.1 A per ADAM step against 0.9 A
+//     cells, so only a few percent of evaluations copy anything;
 //  C  neighbour pairs: the owners write their beads' list entries into the
 //     team's pair buffer, and the team's lanes take the pairs round-robin
 //     (balanced whatever the per-bead list lengths);
@@ -21,8 +22,8 @@
 // so each lane accumulates its own share and the team sums 7 values with
 // xor-shuffles per evaluation.  The rigid-body ADAM step runs on team lanes
 // 0..5 between evaluations; a persistent launch pulls tiles of poses from a
-// work counter.  The kernels hold no spin-wait: every wait is on the issuing
-// thread's own copies or a warp barrier.
+// work counter.  Every mbarrier wait is bounded; a timeout sets the device
+// error word and the warp returns.
 //
 // Semantics follow test5.py (sjdv1982/attract-jax):
 //   transform            [x,1] @ mat                    test5.py:315-317
@@ -656,7 +657,8 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
               float v = 0.f;
               if (c < 3) {
                 if (r < 3) v = acc_t[r * 3 + c];
-                else v = (c == 0) ? acc_gx : (c == 1 ? acc_gy : acc_gz);
+                else v = (c == 0) ? acc_gx + 2.f * p.gravity * tx
+                                  : (c == 1 ? acc_gy + 2.f * p.gravity * ty : acc_gz + 2.f * p.gravity * tz);
               }
               p.grad[(long long)b * 16 + k] = v;
             }

@@ -110,8 +110,6 @@ class Grid:
         rec_type = np.asarray(rec_type, np.int64)
         if len(rec_type) and (rec_type.min() < 0 or rec_type.max() >= ff.n_rtypes):
             raise ValueError("receptor type outside the force field")
-        if geom.n_types > ff.n_ltypes:
-            raise ValueError("grid has more potential slots than the force field has ligand types")
         self.n_rec = len(rec_type)
         self.rec = pack_receptor(rec_xyz, rec_type, self.device)
         self.rec_xyz = np.asarray(rec_xyz, np.float64).reshape(-1, 3)
@@ -247,6 +245,8 @@ class Grid:
         """
         dev = _dev(device)
         lib = _lib.load()
+        if potentials and geom.n_types > ff.n_ltypes:
+            raise ValueError("grid has more potential slots than the force field has ligand types")
         if list_radius is None:
             list_radius = geom.plateau + geom.spacing * np.sqrt(3.0) / 2.0 + 1e-3
         rec = pack_receptor(rec_xyz, rec_type, dev)

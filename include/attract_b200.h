@@ -53,8 +53,7 @@ extern "C" {
 #define ATT_STATUS_NONFINITE_ENERGY 2 /* the returned energy is not finite */
 
 /* device-wide kernel error word (att_kernel_status) */
-#define ATT_KERR_COPY_TIMEOUT 1 /* reserved: a warp gave up waiting for its copies (the current kernels
-                                   wait only on their own asynchronous copies and never set it) */
+#define ATT_KERR_COPY_TIMEOUT 1 /* a warp gave up waiting for its grid-brick / record bulk copies and returned */
 #define ATT_KERR_BOUNDS 2       /* (ATT_BOUNDS_CHECK builds) an index failed its check; the access was skipped */
 
 /* A pose is served by lanes_per_pose lanes holding up to 8 beads each; a
@@ -214,8 +213,8 @@ int att_nbgrid_fill(const AttGridGeom* geom, const float* rec_dev, int n_rec, fl
 /* Fixed-size neighbour records from the CSR lists: record v holds
    {overflow index = start + inline, count, first `inline` entries (rest
    ATT_NB_EMPTY)}; entries beyond the inline ones stay in the CSR list, which
-   the kernels keep reading.  A bead copies its record into shared memory
-   with the same asynchronous copies as its grid brick, every step.
+   the kernels keep reading.  A record is one bulk copy into shared memory,
+   made when a bead's nearest inner grid point changes.
    records_dev: n_voxels * rec_bytes bytes, 16-B aligned; rec_bytes 32/64/128.
    (No counterpart in the reference: a layout of the neighbour grid of
    read_grid2.py:113-124 for the B200 kernels.) */

@@ -391,6 +391,97 @@ def energrad_mat(mat, lig, lig_gtype, lig_ltype, G, mode="reference", quirk=True
     return Eb.astype(np.float64).sum(1), dmat
 
 
+# --------------------------------------------------------------------------
+# quaternion call surface (test5.py:411-429) and the adabelief SCHEMA
+# protocol (test5.py:14-23, 436-467)
+# --------------------------------------------------------------------------
+def _cross_matrix(v):
+    z = np.zeros(v.shape[:-1])
+    x, y, w = v[..., 0], v[..., 1], v[..., 2]
+    return np.stack([np.stack([z, -w, y], -1), np.stack([w, z, -x], -1), np.stack([-y, x, z], -1)], -2)
+
+
+def quat_to_matrix(q):
+    """``Rotation.as_matrix()`` of scalar-last quaternions (the form JAX
+    differentiates): R = (w^2 - v.v) I + 2 v v^T + 2 w [v]x."""
+    q = np.asarray(q, np.float64)
+    v, w = q[..., :3], q[..., 3]
+    return ((w * w - (v * v).sum(-1))[..., None, None] * np.eye(3) + 2.0 * v[..., :, None] * v[..., None, :]
+            + 2.0 * w[..., None, None] * _cross_matrix(v))
+
+
+def quat_grad(q, dEdR):
+    """dE/dq = sum_ij dE/dR_ij dR_ij/dq for :func:`quat_to_matrix`:
+    dR/dw = 2 w I + 2 [v]x;  dR/dv_i = -2 v_i I + 2 (e_i v^T + v e_i^T) + 2 w [e_i]x."""
+    q = np.asarray(q, np.float64)
+    G = np.asarray(dEdR, np.float64)
+    v, w = q[..., :3], q[..., 3]
+    E = np.eye(3)
+    out = np.zeros(q.shape)
+    for i in range(3):
+        ei = np.broadcast_to(E[i], v.shape)
+        dR = (-2.0 * v[..., i][..., None, None] * E + 2.0 * (ei[..., :, None] * v[..., None, :]
+              + v[..., :, None] * ei[..., None, :]) + 2.0 * w[..., None, None] * _cross_matrix(ei))
+        out[..., i] = (G * dR).sum((-2, -1))
+    dRw = 2.0 * w[..., None, None] * E + 2.0 * _cross_matrix(v)
+    out[..., 3] = (G * dRw).sum((-2, -1))
+    return out
+
+
+def energrad_quat(q, t, lig_confs, conformers, lig_gtype, lig_ltype, G, gravity=0.0, mode="reference",
+                  quirk=True, dtype=np.float64):
+    """The reference's ``value_and_grad(main)`` (test5.py:411-429) for
+    quaternion rotations: (E [B], dE/dq [B,4], dE/dt [B,3]).  The quaternion
+    is normalised first (``Rotation.from_quat``); ``conformers`` index
+    ``lig_confs [C,N,3]`` (test5.py:316); gravity*|t|^2 as test5.py:419."""
+    q = np.asarray(q, np.float64)
+    q = q / np.linalg.norm(q, axis=1, keepdims=True)
+    t = np.asarray(t, np.float64)
+    conformers = np.asarray(conformers, np.int64)
+    mat = np.ones((len(q), 4, 4))
+    mat[:, :3, :3] = quat_to_matrix(q)
+    mat[:, 3, :3] = t
+    E = np.zeros(len(q))
+    dmat = np.zeros((len(q), 4, 4))
+    for c in np.unique(conformers):
+        sel = conformers == c
+        E[sel], dmat[sel] = energrad_mat(mat[sel], lig_confs[c], lig_gtype, lig_ltype, G, mode, quirk, dtype)
+    E = E + gravity * (t * t).sum(1)
+    gt = dmat[:, 3, :3] + 2.0 * gravity * t
+    return E, quat_grad(q, dmat[:, :3, :3]), gt
+
+
+def minimise_schema(q, t, lig_confs, conformers, lig_gtype, lig_ltype, G, schema, gravity_weight=0.1,
+                    b1=0.9, b2=0.999, eps=1e-16, eps_root=1e-16, dtype=np.float64):
+    """test5.py:445-463: per stage (epochs, lr, gravity) a fresh
+    optax.adabelief(lr) over (quaternion, translation).  optax's
+    scale_by_belief: m <- b1 m + (1-b1) g;  s <- b2 s + (1-b2) (g - m_prev)^2
+    + eps_root;  update = -lr (m / (1-b1^k)) / (sqrt(s / (1-b2^k)) + eps).
+    After each update the quaternion is renormalised
+    (``Rotation.from_quat(rotations.as_quat())``).  Returns (q, t, E) with E
+    from the last evaluation, as the reference reports it (test5.py:465)."""
+    q = np.array(q, np.float64)
+    q = q / np.linalg.norm(q, axis=1, keepdims=True)
+    t = np.array(t, np.float64)
+    E = None
+    for epochs, lr, grav in schema:
+        mu = [np.zeros_like(q), np.zeros_like(t)]
+        nu = [np.zeros_like(q), np.zeros_like(t)]
+        for k in range(1, int(epochs) + 1):
+            E, gq, gt = energrad_quat(q, t, lig_confs, conformers, lig_gtype, lig_ltype, G,
+                                      gravity_weight if grav else 0.0, dtype=dtype)
+            upd = []
+            for i, g in enumerate((gq, gt)):
+                err = g - mu[i]
+                mu[i] = b1 * mu[i] + (1 - b1) * g
+                nu[i] = b2 * nu[i] + (1 - b2) * err * err + eps_root
+                upd.append(-lr * (mu[i] / (1 - b1 ** k)) / (np.sqrt(nu[i] / (1 - b2 ** k)) + eps))
+            q = q + upd[0]
+            t = t + upd[1]
+            q = q / np.linalg.norm(q, axis=1, keepdims=True)
+    return q, t, E
+
+
 def allpairs_energy(pose, lig, lig_ltype, rec, rtype, pair, rcut2=None):
     """Explicit all-pairs ATTRACT energy (test-energy.py:46-58; ATTRACT --rcut)."""
     X = transform(np.atleast_2d(pose), np.asarray(lig, np.float64))

@@ -1,0 +1,128 @@
+"""The reference's call surface (attract_b200.reference_api: main, vgrad_main,
+minimise_schema) against the oracle's restatement of test5.py, with the
+receptor grid passed the reference's way: ATTRACT .grid bytes read by
+read_grid(data, read_gradients=True).
+
+Tolerances as in test_gpu_parity.py: energies 1e-5 of the sum of |terms|
+(plus float32 position rounding, the force field being uncapped as the
+reference's is); gradients five times the float32 oracle's own deviation plus
+1e-4 of the sum of |gradient terms|."""
+import numpy as np
+import pytest
+import torch
+
+import attract_oracle as O
+from gpu_cases import oracle_scales, small_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(seed=60, n_poses=64):
+    from scipy.spatial.transform import Rotation
+
+    from attract_b200 import load_library
+    from attract_b200.gridfile import read_grid, write_grid
+    from attract_b200.reference_api import make_ff
+
+    load_library()
+    c = small_case(seed=seed, n_poses=n_poses, cap=False)  # the reference's force field has no cap
+    G, g = c["G"], c["G"]["geom"]
+    alphabet = np.zeros(99, bool)
+    alphabet[[2, 7, 11, 20][: c["n_types"]]] = True
+    data = write_grid(gridspacing=g["spacing"], gridextension=g["extension"], plateaudis=g["plateau"],
+                      neighbourdis=g["plateau"] + 1.0, alphabet=alphabet, origin=g["origin"], dim=g["dim"],
+                      dim2=g["dim2"], natoms=len(G["rec"]), inner_potential_grid=G["inner"],
+                      outer_potential_grid=G["outer"], nb_hdr=G["nb_hdr"], nb_list=G["nb_list"])
+    grid = read_grid(data, read_gradients=True)
+    rng = np.random.default_rng(seed + 1)
+    lig2 = c["lig"] + rng.normal(scale=0.3, size=c["lig"].shape).astype(np.float32)
+    confs = np.stack([c["lig"], lig2])
+    conformers = rng.integers(0, 2, n_poses)
+    q = Rotation.from_matrix(O.pose_to_mat(c["poses"])[:, :3, :3]).as_quat()
+    t = c["poses"][:, 3:6].copy()
+    args = dict(coor_rec=G["rec"].astype(np.float32), rec_atomtypes=G["rtype"], coor_lig=confs.astype(np.float32),
+                lig_atomtypes=c["lt"], conformers=conformers, lig_atomtype_pos=c["gt"],
+                ff=make_ff(c["rc"], c["ac"], c["ivor"]), grid=grid)
+    es = np.zeros(n_poses)
+    gs = np.zeros(n_poses)
+    for k in (0, 1):
+        e, s = oracle_scales(dict(c, lig=confs[k]), c["poses"], position_term=True)
+        es = np.where(conformers == k, e, es)
+        gs = np.where(conformers == k, s, gs)
+    es = es + 0.1 * (t * t).sum(1)
+    return c, q, t, confs, conformers, args, es, gs
+
+
+@pytest.fixture(scope="module")
+def setup():
+    return _setup()
+
+
+def test_vgrad_main_matches_oracle(setup):
+    from attract_b200.reference_api import vgrad_main
+
+    c, q, t, confs, conformers, args, es, gs = setup
+    (tot, E), (gq, gt) = vgrad_main(q, t, **args, gravity=True)
+    E, gq, gt = E.cpu().numpy(), gq.cpu().numpy(), gt.cpu().numpy()
+    Eo, gqo, gto = O.energrad_quat(q, t, confs, conformers, c["gt"], c["lt"], c["G"], gravity=0.1)
+    _, gq32, gt32 = O.energrad_quat(q, t, confs, conformers, c["gt"], c["lt"], c["G"], gravity=0.1,
+                                    dtype=np.float32)
+    assert np.all(np.abs(E - Eo) <= 1e-5 * es + 1e-4)
+    assert abs(float(tot) - Eo.sum()) <= 1e-5 * es.sum() + 1e-3
+    assert np.all(np.abs(gt - gto) <= 5 * np.abs(gt32 - gto) + 1e-4 * gs[:, None] + 1e-3)
+    # dE/dq sums the 9 entries of dE/dR times 2|q| <= 2: its scale is 6 * gs
+    assert np.all(np.abs(gq - gqo) <= 5 * np.abs(gq32 - gqo) + 6e-4 * gs[:, None] + 1e-3)
+
+
+def test_main_matrices_and_no_gravity(setup):
+    from scipy.spatial.transform import Rotation
+
+    from attract_b200.reference_api import main
+
+    c, q, t, confs, conformers, args, es, gs = setup
+    R = Rotation.from_quat(q).as_matrix()
+    tot, E = main(R, t, **args, gravity=False)
+    Eo, _, _ = O.energrad_quat(q, t, confs, conformers, c["gt"], c["lt"], c["G"], gravity=0.0)
+    es0 = es - 0.1 * (t * t).sum(1)
+    assert np.all(np.abs(E.cpu().numpy() - Eo) <= 1e-5 * es0 + 1e-4)
+
+
+def test_single_conformer_and_errors(setup):
+    from attract_b200.reference_api import main, vgrad_main
+
+    c, q, t, confs, conformers, args, es, gs = setup
+    one = dict(args, coor_lig=confs[0], conformers=None)
+    _, E = main(q, t, **one, gravity=True)
+    Eo, _, _ = O.energrad_quat(q, t, confs[:1], np.zeros(len(q), int), c["gt"], c["lt"], c["G"], gravity=0.1)
+    e0, _ = oracle_scales(c, c["poses"], position_term=True)
+    assert np.all(np.abs(E.cpu().numpy() - Eo) <= 1e-5 * (e0 + 0.1 * (t * t).sum(1)) + 1e-4)
+    with pytest.raises(AssertionError):
+        main(q, t[:-1], **args, gravity=True)  # test5.py:412
+    with pytest.raises(AssertionError):
+        main(q, t, **dict(args, conformers=np.full(len(q), 2)), gravity=True)
+    with pytest.raises(AssertionError):
+        vgrad_main(np.zeros((len(q), 3, 3)), t, **args, gravity=True)
+
+
+def test_schema_minimisation_reproduces_the_oracle_ranking():
+    """A shortened SCHEMA (two stages, gravity then none) on poses without
+    deep clashes: the float32 CUDA path follows the float64 oracle's
+    trajectories, so final energies and their ranking agree."""
+    from scipy.stats import spearmanr
+
+    from attract_b200.reference_api import minimise_schema
+
+    c, q, t, confs, conformers, args, es, gs = _setup(seed=61, n_poses=96)
+    Eo0, _, _ = O.energrad_quat(q, t, confs, conformers, c["gt"], c["lt"], c["G"])
+    keep = Eo0 < 1e3  # start outside deep clashes, where the uncapped 8-6 term is steep
+    q, t, conformers = q[keep], t[keep], conformers[keep]
+    args = dict(args, conformers=conformers)
+    schema = ((4, 0.5, True), (6, 0.05, False))
+    qg, tg, Eg = minimise_schema(q, t, **args, schema=schema)
+    qo, to, Eo = O.minimise_schema(q, t, confs, conformers, c["gt"], c["lt"], c["G"], schema)
+    Eg = Eg.cpu().numpy()
+    assert np.all(np.isfinite(Eg))
+    rho = spearmanr(Eg, Eo)[0]
+    assert rho > 0.98, rho
+    close = np.abs(Eg - Eo) <= 1e-3 * np.abs(Eo) + 1e-2
+    assert close.mean() >= 0.9, close.mean()

@@ -14,6 +14,7 @@ import os
 import numpy as np
 import torch
 
+from ._lib import AttractError
 from .engine import AdamOptions, EvalOptions, LaunchShape, Segment, Workload, minimise
 
 CANDIDATES = [(8, 64), (8, 128), (16, 64), (16, 128), (32, 64), (32, 128)]
@@ -54,7 +55,12 @@ def autotune(wl: Workload, poses: torch.Tensor, steps: int = 10, sample: int = 6
     for lanes, threads in candidates:
         w = Workload(wl.grids, wl.ligands, segs, lanes, wl.device)
         shape = LaunchShape(lanes, threads)
-        minimise(w, sp, 1, adam, opts, launch=shape)  # warm
+        try:
+            minimise(w, sp, 1, adam, opts, launch=shape)  # warm
+        except AttractError as e:
+            if "shared memory" not in str(e):
+                raise
+            continue  # this block size cannot hold the beads per lane this ligand mix needs
         best = float("inf")
         for _ in range(repeats):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -64,6 +70,8 @@ def autotune(wl: Workload, poses: torch.Tensor, steps: int = 10, sample: int = 6
             torch.cuda.synchronize()
             best = min(best, a.elapsed_time(b))
         times[f"{lanes}x{threads}"] = best
+    if not times:
+        raise AttractError("no candidate launch shape fits this workload's shared memory")
     lanes, threads = (int(x) for x in min(times, key=times.get).split("x"))
     if use_cache:
         try:

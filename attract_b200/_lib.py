@@ -86,6 +86,7 @@ SIGNATURES = {
     "att_nbgrid_count_noalloc": (I, [C.POINTER(AttGridGeom), P, I, F, P, P, P]),
     "att_nbgrid_pack_records": (I, [P, P, LL, I, P, P]),
     "att_kernel_debug_info": (I, [C.POINTER(C.c_ulonglong), I, P]),
+    "att_allpairs_energy": (I, [P, I, P, I, P, I, I, P, I, I, F, P, P, P]),
 }
 
 _lib = None

@@ -240,6 +240,20 @@ int att_nbgrid_pack_records(const uint32_t* hdr_dev, const uint16_t* list_dev, l
 int att_nbgrid_count_noalloc(const AttGridGeom* geom, const float* rec_dev, int n_rec, float radius,
                              uint32_t* hdr_dev, unsigned long long* total_dev, void* stream);
 
+/* Explicit all-pairs ATTRACT energy without grids: for every pose, the sum
+   over every (ligand bead, receptor bead) pair with d < rcut (rcut = 0: all
+   pairs) of the pair potential of `pair_dev` (same layout as AttGrid.pair;
+   give it eplat = 0 for the plain potential).  rec_dev [n_rec][4] x, y, z,
+   receptor type (int32 bits); lig_dev [n_lig][4] x, y, z, ligand type (int32
+   bits); pose_dev [B][6] (pose_format 0) or [B][16] row-vector 4x4 (1);
+   energy_dev [B]; grad_dev [B][6] dE/d(Euler, t) or [B][16] dE/dmat, may be
+   NULL.  Replaces main() of test-energy.py:46-58 (the reference's rescoring;
+   ATTRACT --score with --rcut). */
+int att_allpairs_energy(const float* rec_dev, int n_rec, const float* lig_dev, int n_lig,
+                        const float* pose_dev, int n_poses, int pose_format, const float* pair_dev,
+                        int n_rtypes, int n_ltypes, float rcut, float* energy_dev, float* grad_dev,
+                        void* stream);
+
 /* Read the device-wide error word of the scoring kernels (ATT_KERR_* bits, 0 =
    none) into *error_word, clearing it if `clear`; synchronises `stream`.  A
    non-zero word means some warp stopped early and its poses' outputs are stale.

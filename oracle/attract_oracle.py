@@ -482,6 +482,42 @@ def minimise_schema(q, t, lig_confs, conformers, lig_gtype, lig_ltype, G, schema
     return q, t, E
 
 
+def allpairs_energrad(pose, lig, lig_ltype, rec, rtype, pair, rcut2=None, bead_grad=False):
+    """Explicit all-pairs energy with its pose gradient: test-energy.py:46-58's
+    sum of nonbon over every (ligand, receptor) pair within ``rcut2``, and the
+    chain rule of :func:`energrad` (dE/dt = sum_b g_b, dE/d(angle_k) = w_k .
+    sum_b (x_b - t) x g_b, g_b = sum_j 2 dnonbon/d(d^2) d_bj).  Also returns
+    the per-pose sums of |energy term| and |gradient term| (1 + |x_b - t|),
+    the float32 error scales of the parity tests.  Returns (E, grad, e_abs, g_abs),
+    plus the per-bead dE/dx [B,N,3] with ``bead_grad``."""
+    pose = np.atleast_2d(np.asarray(pose, np.float64))
+    X = transform(pose, np.asarray(lig, np.float64))
+    rec = np.asarray(rec, np.float64)
+    prm = _pp(pair, np.asarray(lig_ltype)[:, None], np.asarray(rtype)[None, :])
+    rc, ac, emin, rmin2, ivor, eplat, _, rcap2 = (np.asarray(v, np.float64) for v in prm)
+    t = pose[:, 3:6]
+    E = np.zeros(len(pose))
+    ea = np.zeros(len(pose))
+    ga = np.zeros(len(pose))
+    gb = np.zeros_like(X)
+    for b in range(len(pose)):
+        d = X[b][:, None, :] - rec[None]
+        dsq = (d * d).sum(-1)
+        keep = np.ones_like(dsq, bool) if rcut2 is None else dsq < rcut2
+        e = np.where(keep, nonbon(dsq, rc, ac, emin, rmin2, ivor, rcap2) - eplat, 0.0)
+        g = np.where(keep, dnonbon_ddsq(dsq, rc, ac, emin, rmin2, ivor, rcap2), 0.0)
+        E[b] = e.sum()
+        ea[b] = np.abs(e).sum()
+        gvec = 2.0 * g[..., None] * d
+        gb[b] = gvec.sum(1)
+        arm = 1.0 + np.linalg.norm(X[b] - t[b], axis=1)
+        ga[b] = (np.abs(gvec).sum((1, 2)) * arm).sum()
+    tau = np.cross(X - t[:, None, :], gb).sum(1)
+    W = euler_axes(pose[:, 0], pose[:, 1])
+    grad = np.concatenate([np.einsum("bkj,bj->bk", W, tau), gb.sum(1)], 1)
+    return (E, grad, ea, ga, gb) if bead_grad else (E, grad, ea, ga)
+
+
 def allpairs_energy(pose, lig, lig_ltype, rec, rtype, pair, rcut2=None):
     """Explicit all-pairs ATTRACT energy (test-energy.py:46-58; ATTRACT --rcut)."""
     X = transform(np.atleast_2d(pose), np.asarray(lig, np.float64))

@@ -99,7 +99,7 @@ def load(path: str | None = None):
     if _lib is not None:
         return _lib
     if path is None:
-        path = os.environ.get("ATTRACT_B200_LIB", LIB_PATH)
+        path = os.environ.get("ATTRACT_B200_LIB") or LIB_PATH
     if not os.path.exists(path):
         raise AttractError(
             f"{path} is missing: build it with `python -m attract_b200.build` (nvcc, sm_100a); "

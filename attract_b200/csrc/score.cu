@@ -559,7 +559,9 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
               const BeadPos bp = bpos[bi];
               float px, py, pz;
               pair_term_masked(p, G, bp, rr[m], acc_e, px, py, pz);
-              const BeadArm ba = barm[bi];
+              BeadArm ba;  // lever arm: Q x = X - t (the 4x4 form needs the ligand-frame x)
+              if (MAT) ba = barm[bi];
+              else { ba.x = bp.x - tx; ba.y = bp.y - ty; ba.z = bp.z - tz; }
               acc_gx += px;
               acc_gy += py;
               acc_gz += pz;

@@ -99,11 +99,34 @@ def pack_receptor(xyz, rtype, device) -> torch.Tensor:
     return torch.from_numpy(a).to(device)
 
 
+def spatial_order(xyz, bits: int = 10) -> np.ndarray:
+    """Permutation putting points in Morton (Z-curve) order of their position
+    quantised to 2**bits cells per axis of the bounding box."""
+    x = np.asarray(xyz, np.float64).reshape(-1, 3)
+    if len(x) == 0:
+        return np.zeros(0, np.int64)
+    lo = x.min(0)
+    span = max(float(np.ptp(x, 0).max()), 1e-9)
+    q = np.minimum(((x - lo) / span * ((1 << bits) - 1) + 0.5).astype(np.int64), (1 << bits) - 1)
+    code = np.zeros(len(x), np.int64)
+    for b in range(bits):
+        for k in range(3):
+            code |= ((q[:, k] >> b) & 1) << (3 * b + k)
+    return np.argsort(code, kind="stable")
+
+
 class Grid:
-    """One receptor (potential grids + neighbour grid + beads) on the device."""
+    """One receptor (potential grids + neighbour grid + beads) on the device.
+
+    The receptor beads are held on the device in Morton order of their
+    positions (``rec_perm``: device position -> given index), and the
+    neighbour lists name beads by device position: the beads one warp's
+    lists name then share few cache lines.  ``rec_xyz``/``rec_type`` and
+    :meth:`dense_host` keep the caller's order.
+    """
 
     def __init__(self, geom: GridGeom, rec_xyz, rec_type, ff: ForceField, *, bricks=None, nb_hdr=None,
-                 nb_list=None, inner=None, outer=None, shift_plateau=None, device=None):
+                 nb_list=None, inner=None, outer=None, shift_plateau=None, device=None, list_space="given"):
         self.device = _dev(device)
         self.geom = geom
         self.ff = ff
@@ -111,9 +134,16 @@ class Grid:
         if len(rec_type) and (rec_type.min() < 0 or rec_type.max() >= ff.n_rtypes):
             raise ValueError("receptor type outside the force field")
         self.n_rec = len(rec_type)
-        self.rec = pack_receptor(rec_xyz, rec_type, self.device)
         self.rec_xyz = np.asarray(rec_xyz, np.float64).reshape(-1, 3)
         self.rec_type = rec_type
+        self.rec_perm = spatial_order(self.rec_xyz)
+        self.rec = pack_receptor(self.rec_xyz[self.rec_perm], rec_type[self.rec_perm], self.device)
+        if nb_list is not None and list_space == "given" and self.n_rec:
+            lut = torch.full((1 << 16,), _lib.ATT_NB_EMPTY, dtype=torch.int32, device=self.device)
+            inv = np.empty(self.n_rec, np.int64)
+            inv[self.rec_perm] = np.arange(self.n_rec)
+            lut[: self.n_rec] = torch.from_numpy(inv.astype(np.int32)).to(self.device)
+            nb_list = lut[nb_list.to(torch.int64) & 0xFFFF].to(torch.int16)
         self.bricks = bricks
         self.inner = inner
         self.outer = outer
@@ -249,7 +279,8 @@ class Grid:
             raise ValueError("grid has more potential slots than the force field has ligand types")
         if list_radius is None:
             list_radius = geom.plateau + geom.spacing * np.sqrt(3.0) / 2.0 + 1e-3
-        rec = pack_receptor(rec_xyz, rec_type, dev)
+        perm = spatial_order(rec_xyz)  # the order Grid.__init__ puts the beads in
+        rec = pack_receptor(np.asarray(rec_xyz, np.float64).reshape(-1, 3)[perm], np.asarray(rec_type)[perm], dev)
         n_rec = len(np.asarray(rec_type).reshape(-1))
         gc = geom.to_c()
         with torch.cuda.device(dev):
@@ -282,7 +313,7 @@ class Grid:
                                            _lib.ptr(lst), st), "att_nbgrid_fill")
         g = cls(geom, rec_xyz, rec_type, ff, bricks=bricks, nb_hdr=hdr, nb_list=lst,
                 inner=inner_t if keep_dense else None, outer=outer_t if keep_dense else None,
-                shift_plateau=potentials, device=dev)
+                shift_plateau=potentials, device=dev, list_space="device")
         g.list_radius = list_radius
         g.cutoff = cutoff
         return g
@@ -291,10 +322,28 @@ class Grid:
         return 0 if self.nb_list is None else self.nb_list.numel()
 
     def dense_host(self):
-        """(inner, outer, nb_hdr, nb_list) as NumPy arrays (for checks)."""
+        """(inner, outer, nb_hdr, nb_list) as NumPy arrays (for checks), the
+        lists naming beads by the caller's index, ascending per grid point."""
         f = lambda t: None if t is None else t.detach().cpu().numpy()
         hdr = None if self.nb_hdr is None else f(self.nb_hdr).view(np.uint32)
-        lst = None if self.nb_list is None else f(self.nb_list).view(np.uint16)
+        lst = None if self.nb_list is None else f(self.nb_list).view(np.uint16).copy()
+        if lst is not None and self.n_rec:
+            total = int(hdr[:, 1].astype(np.int64).sum())
+            body = lst[:total].astype(np.int64)
+            ok = body < self.n_rec
+            body[ok] = self.rec_perm[body[ok]]
+            body[~ok] = _lib.ATT_NB_EMPTY
+            vox = np.repeat(np.arange(len(hdr)), hdr[:, 1].astype(np.int64))
+            start = hdr[:, 0].astype(np.int64)
+            if np.array_equal(start, np.cumsum(hdr[:, 1].astype(np.int64)) - hdr[:, 1]):
+                lst[:total] = body[np.lexsort((body, vox))]
+            else:  # general CSR: sort each list in place
+                for v in np.flatnonzero(hdr[:, 1]):
+                    s0, n = int(start[v]), int(hdr[v, 1])
+                    vals = lst[s0:s0 + n].astype(np.int64)
+                    ok = vals < self.n_rec
+                    vals[ok] = self.rec_perm[vals[ok]]
+                    lst[s0:s0 + n] = np.sort(vals)
         return f(self.inner), f(self.outer), hdr, lst
 
 

@@ -285,6 +285,19 @@ def other_configs(args, device, shape):
         docking_energy(wl, P, A.EvalOptions(grad_mode="analytic")).backward()
 
     ms = _timed(fwd_bwd, 10)
+    # explicit all-pairs rescoring of the same poses (no grids): 2500 x 24 pairs per pose
+    from attract_b200.allpairs import AllPairs
+
+    lig = cfg.ligands[0]
+    ap = AllPairs(cfg.rec_xyz, cfg.rec_type, lig[0], lig[2], cfg.ff, device=device)
+    Pd = P.detach()
+    ms_ap = _timed(lambda: ap.energy(Pd, grad=True), 5)
+    n_pairs = len(cfg.rec_type) * len(lig[0]) * wl.n_poses
+    res["allpairs"] = {"workload": "explicit all-pairs rescoring with gradient: config-1 receptor (2500 beads) x "
+                                   "24-bead ligand x 65536 poses", "ms": round(ms_ap, 3),
+                       "value": round(wl.n_poses / ms_ap * 1e3, 1), "unit": "poses/s",
+                       "pairs_per_s": round(n_pairs / ms_ap * 1e3, 1)}
+    del ap
     res["config3"] = {"workload": "differentiation: config-1 receptor, 24-bead ligand, 65536 poses, summed energy, "
                                   "backward to poses and grid energies (analytic mode)",
                       "poses": wl.n_poses, "ms_forward_backward": round(ms, 3),

@@ -110,8 +110,8 @@ __global__ void __launch_bounds__(ALLPAIRS_THREADS) allpairs_kernel(const __grid
             const float dx = X - r.x, dy = Y - r.y, dz = Z - r.z;
             const float dsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const bool hit = ((unsigned)rt < (unsigned)p.n_rtypes) & ((p.rcut2 <= 0.f) | (dsq < p.rcut2));
-            const float4 p0 = __ldg(prow + (hit ? rt : 0) * 2);      // rc, ac, emin, rmin2
-            const float4 p1 = __ldg(prow + (hit ? rt : 0) * 2 + 1);  // ivor, eplat, -, rcap2
+            float4 p0, p1;  // rc, ac, emin, rmin2 / ivor, eplat, -, rcap2
+            ldg_f4x2(prow + (hit ? rt : 0) * 2, p0, p1);
             const float d2 = fmaxf(dsq, p1.w);
             const float rr2 = 1.0f / d2;
             const float rr6 = rr2 * rr2 * rr2;
@@ -189,8 +189,8 @@ extern "C" int att_allpairs_energy(const float* rec_dev, int n_rec, const float*
   if (pose_format != 0 && pose_format != 1) return bad("att_allpairs_energy: pose_format must be 0 or 1");
   if ((n_rec && !rec_dev) || !lig_dev || !pair_dev || (n_poses && (!pose_dev || !energy_dev)))
     return bad("att_allpairs_energy: NULL buffer");
-  if ((rec_dev && !al16(rec_dev)) || !al16(lig_dev) || !al16(pair_dev))
-    return bad("att_allpairs_energy: receptor, ligand and pair table must be 16-byte aligned");
+  if ((rec_dev && !al16(rec_dev)) || !al16(lig_dev) || (reinterpret_cast<uintptr_t>(pair_dev) & 31u))
+    return bad("att_allpairs_energy: receptor and ligand must be 16-byte, the pair table 32-byte aligned");
   if (!(rcut >= 0.f)) return bad("att_allpairs_energy: rcut must be >= 0 (0 = no cutoff)");
   if (n_poses == 0) return ATT_OK;
   AllPairsParams p;

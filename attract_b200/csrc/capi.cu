@@ -92,7 +92,7 @@ static int make_kgrid(const AttGrid* a, int gi, KGrid* k) {
   REQUIRE(a->n_rec >= 0 && a->n_rec < (int)ATT_NB_EMPTY, "grid %d: n_rec = %d out of range [0, 65535)", gi,
           a->n_rec);
   REQUIRE(a->n_rec == 0 || (a->rec != nullptr && aligned(a->rec, 16)), "grid %d: rec NULL or not 16-B aligned", gi);
-  REQUIRE(aligned(a->pair, 16), "grid %d: pair table not 16-B aligned", gi);
+  REQUIRE(aligned(a->pair, 32), "grid %d: pair table not 32-B aligned", gi);
   if (a->bricks != nullptr) {
     REQUIRE(aligned(a->bricks, 128), "grid %d: bricks must be 128-B aligned", gi);
     REQUIRE(a->n_inner_bricks == ni, "grid %d: n_inner_bricks = %lld, expected %lld", gi, a->n_inner_bricks, ni);

@@ -175,9 +175,8 @@ __device__ __forceinline__ void pair_term_masked(const KParams& p, const KGrid& 
   const bool hit =
       (dsq < G.plateau2) & ((unsigned)rt < (unsigned)G.n_rtypes) & ((unsigned)bp.lt < (unsigned)G.n_ltypes);
   const int idx = hit ? bp.lt * G.n_rtypes + rt : 0;
-  const float4* pp = G.pair + (long long)idx * 2;
-  const float4 p0 = ldg_f4(pp);      // rc, ac, emin, rmin2
-  const float4 p1 = ldg_f4(pp + 1);  // ivor, eplat, gplat, rcap2
+  float4 p0, p1;  // rc, ac, emin, rmin2 / ivor, eplat, gplat, rcap2: one 32-B row
+  ldg_f4x2(G.pair + (long long)idx * 2, p0, p1);
   const float d2 = fmaxf(dsq, p1.w);
   float rr2;  // approximate reciprocal (1 ulp): the pair energy carries ~4 ulp
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rr2) : "f"(d2));

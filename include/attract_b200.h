@@ -89,7 +89,7 @@ typedef struct AttGrid {
   int n_rtypes;                /* receptor types in the pair table */
   int n_ltypes;                /* ligand types in the pair table */
   int nb_rec_bytes;            /* 32, 64 or 128: size of one neighbour record (below) */
-  const float* pair;           /* [n_ltypes][n_rtypes][8]: rc, ac, emin, rmin2, ivor, eplat, gplat, rcap2 */
+  const float* pair;           /* [n_ltypes][n_rtypes][8], 32-B aligned: rc, ac, emin, rmin2, ivor, eplat, gplat, rcap2 */
   const void* nb_rec;          /* [dim0*dim1*dim2] neighbour records, 16-B aligned (att_nbgrid_pack_records):
                                   u32 overflow index into nb_list, u16 count, then the first
                                   (nb_rec_bytes - 6) / 2 entries inline; required with nb_hdr */

@@ -36,7 +36,7 @@ class AttGrid(C.Structure):
                 ("n_outer_bricks", C.c_longlong), ("nb_hdr", C.c_void_p), ("nb_list", C.c_void_p),
                 ("n_nb_entries", C.c_longlong), ("rec", C.c_void_p), ("n_rec", C.c_int),
                 ("n_rtypes", C.c_int), ("n_ltypes", C.c_int), ("nb_rec_bytes", C.c_int), ("pair", C.c_void_p),
-                ("nb_rec", C.c_void_p)]
+                ("nb_rec", C.c_void_p), ("nb_refine", C.c_int), ("pad2_", C.c_int)]
 
 
 class AttLigands(C.Structure):

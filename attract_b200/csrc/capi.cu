@@ -108,6 +108,8 @@ static int make_kgrid(const AttGrid* a, int gi, KGrid* k) {
     REQUIRE(a->nb_rec != nullptr && aligned(a->nb_rec, 16), "grid %d: nb_rec NULL or not 16-B aligned", gi);
     REQUIRE(a->nb_rec_bytes == 32 || a->nb_rec_bytes == 64 || a->nb_rec_bytes == 128,
             "grid %d: nb_rec_bytes = %d (32, 64 or 128)", gi, a->nb_rec_bytes);
+    REQUIRE(a->nb_refine >= 0 && a->nb_refine <= 4 && a->nb_refine != 3, "grid %d: nb_refine = %d (0, 1, 2 or 4)",
+            gi, a->nb_refine);
   }
   memset(k, 0, sizeof(*k));
   k->ox = g.origin[0];
@@ -137,7 +139,11 @@ static int make_kgrid(const AttGrid* a, int gi, KGrid* k) {
   k->type_stride = ni + (k->has_outer ? a->n_outer_bricks : 0);
   k->n_inner = ni;
   k->n_list = a->n_nb_entries;
-  k->n_vox = (long long)g.dim[0] * g.dim[1] * g.dim[2];
+  const int rf = a->nb_refine > 1 ? a->nb_refine : 1;  // list grid = inner grid refined rf times
+  k->nb_scale = (float)rf;
+  k->ndy = (g.dim[1] - 1) * rf + 1;
+  k->ndz = (g.dim[2] - 1) * rf + 1;
+  k->n_vox = (long long)((g.dim[0] - 1) * rf + 1) * k->ndy * k->ndz;
   k->n_bricks = (long long)g.n_types * k->type_stride;
   k->bricks = reinterpret_cast<const float4*>(a->bricks);
   k->nb_hdr = reinterpret_cast<const uint2*>(a->nb_hdr);

@@ -28,6 +28,8 @@ struct __align__(16) KGrid {
   const unsigned char* nb_rec;    // fixed-size records, one per inner grid point
   int nb_rec_bytes;               // record size
   int nb_inline;                  // entries held inline in a record
+  float nb_scale;                 // list-grid points per inner spacing (1, 2 or 4)
+  int ndy, ndz;                   // list-grid points along y and z
   long long n_list;               // CSR entries, records (= inner grid points), bricks (all types):
   long long n_vox;                //   sizes for the bounds checks of ATT_BOUNDS_CHECK builds
   long long n_bricks;

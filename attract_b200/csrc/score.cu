@@ -417,8 +417,10 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
                     : 0;
         nvox[k] = -1;
         if (inn && G.nb_rec != nullptr && lt < G.n_ltypes) {
-          const int nx = (int)floorf(vx + 0.5f), my = (int)floorf(vy + 0.5f), mz = (int)floorf(vz + 0.5f);
-          nvox[k] = ((long long)nx * G.dy + my) * G.dz + mz;
+          // nearest list-grid point (the inner grid point itself when nb_scale = 1)
+          const int nx = (int)floorf(fmaf(vx, G.nb_scale, 0.5f)), my = (int)floorf(fmaf(vy, G.nb_scale, 0.5f)),
+                    mz = (int)floorf(fmaf(vz, G.nb_scale, 0.5f));
+          nvox[k] = ((long long)nx * G.ndy + my) * G.ndz + mz;
         }
         if (use[k] && !ATT_CHECK(bidx[k] >= 0 && bidx[k] < G.n_bricks, 1, bidx[k], G.n_bricks)) use[k] = false;
         if (nvox[k] >= 0 && !ATT_CHECK(nvox[k] < G.n_vox, 2, nvox[k], G.n_vox)) nvox[k] = -1;

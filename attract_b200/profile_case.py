@@ -1,7 +1,7 @@
 """Run the batched minimiser on a synthetic workload a few times (for profilers).
 
     python -m attract_b200.profile_case [--config 1] [--scale 0.05] [--types 32]
-        [--launches 3] [--lanes 32] [--threads 64] [--steps N]
+        [--launches 3] [--lanes 32] [--threads 64] [--steps N] [--refine 2]
 
 Builds the workload (grid build, neighbour lists, bricks), then launches the
 persistent minimisation kernel ``--launches`` times and prints the mean time of
@@ -26,6 +26,7 @@ def main():
     ap.add_argument("--lanes", type=int, default=32)
     ap.add_argument("--threads", type=int, default=64)
     ap.add_argument("--steps", type=int, default=-1)
+    ap.add_argument("--refine", type=int, default=2, help="neighbour-list grid refinement (1, 2 or 4)")
     a = ap.parse_args()
 
     import attract_b200 as A
@@ -34,7 +35,7 @@ def main():
     A.load_library()
     cfg = synth.make_config(a.config, seed=0, scale=a.scale, n_types=a.types)
     steps = cfg.steps if a.steps < 0 else a.steps
-    grid = A.Grid.build(cfg.rec_xyz, cfg.rec_type, cfg.ff, cfg.geom, cutoff=cfg.cutoff)
+    grid = A.Grid.build(cfg.rec_xyz, cfg.rec_type, cfg.ff, cfg.geom, cutoff=cfg.cutoff, nb_refine=a.refine)
     ligs = A.LigandSet(cfg.ligands)
     order = sorted(range(len(cfg.ligands)), key=lambda i: -len(cfg.ligands[i][0]))
     wl = A.Workload([grid], ligs, [A.Segment(0, i, len(cfg.poses[i])) for i in order], lanes_per_pose=a.lanes)

@@ -168,7 +168,7 @@ def cpu_baseline(cfg, grid, order, n_per_frag, steps):
     import attract_oracle as O
 
     inner, outer, hdr, lst = grid.dense_host()
-    G = dict(geom=cfg.geom.as_dict(), inner=inner, outer=outer, nb_hdr=hdr, nb_list=lst,
+    G = dict(geom=dict(cfg.geom.as_dict(), nb_refine=grid.nb_refine), inner=inner, outer=outer, nb_hdr=hdr, nb_list=lst,
              rec=np.asarray(cfg.rec_xyz, np.float32), rtype=cfg.rec_type,
              pair=O.pair_table(cfg.ff.rc, cfg.ff.ac, cfg.ff.ivor, cfg.geom.plateau, True, cfg.ff.rcap2))
     t = time.perf_counter()

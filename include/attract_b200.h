@@ -80,8 +80,8 @@ typedef struct AttGrid {
                                   NULL = no potential grid (neighbour grid only) */
   long long n_inner_bricks;    /* (dim[0]-1)(dim[1]-1)(dim[2]-1) */
   long long n_outer_bricks;    /* (dim2[0]-1)(dim2[1]-1)(dim2[2]-1), 0 = no outer grid */
-  const uint32_t* nb_hdr;      /* [dim0*dim1*dim2][2] = {start, count} per inner grid point (CSR);
-                                  NULL = no neighbour grid */
+  const uint32_t* nb_hdr;      /* [list-grid points][2] = {start, count} per point (CSR; the list grid
+                                  is the inner grid unless nb_refine > 1); NULL = no neighbour grid */
   const uint16_t* nb_list;     /* receptor bead index per entry (ATT_NB_EMPTY skipped) */
   long long n_nb_entries;
   const float* rec;            /* [n_rec][4] x, y, z, receptor type (as an int32 bit pattern) */
@@ -90,9 +90,19 @@ typedef struct AttGrid {
   int n_ltypes;                /* ligand types in the pair table */
   int nb_rec_bytes;            /* 32, 64 or 128: size of one neighbour record (below) */
   const float* pair;           /* [n_ltypes][n_rtypes][8], 32-B aligned: rc, ac, emin, rmin2, ivor, eplat, gplat, rcap2 */
-  const void* nb_rec;          /* [dim0*dim1*dim2] neighbour records, 16-B aligned (att_nbgrid_pack_records):
-                                  u32 overflow index into nb_list, u16 count, then the first
-                                  (nb_rec_bytes - 6) / 2 entries inline; required with nb_hdr */
+  const void* nb_rec;          /* one neighbour record per list-grid point, 16-B aligned
+                                  (att_nbgrid_pack_records): u32 overflow index into nb_list, u16
+                                  count, then the first (nb_rec_bytes - 6) / 2 entries inline;
+                                  required with nb_hdr */
+  int nb_refine;               /* 0 or 1: the lists sit at the inner grid points (the reference's
+                                  neighbour grid); 2 or 4: at the points of the inner grid refined
+                                  that many times per axis (spacing / r, (dim - 1) * r + 1 points per
+                                  axis, same origin), which nb_hdr and nb_rec then index.  A bead
+                                  inside the inner grid reads the list of its nearest list-grid
+                                  point; lists that hold every receptor bead within plateau + the
+                                  list spacing * sqrt(3) / 2 give the same pairs at every r, with
+                                  fewer entries beyond the plateau for larger r. */
+  int pad2_;
 } AttGrid;
 
 /* Inline entries of a neighbour record of `bytes` bytes. */

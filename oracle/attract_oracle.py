@@ -289,7 +289,10 @@ def nb_energrad(pos, ltype, geom, nb_hdr, nb_list, rec, rtype, pair, mode="refer
     the gradient of the custom JVP, ``2 d (dnonbon - gplat * p/|d|)``
     (test5.py:220-229).  ``mode='analytic'`` drops the plateau correction of
     the gradient (the exact derivative of the energy).  ``nb_hdr`` is
-    ``[n_voxels, 2]`` (start, count) into ``nb_list``.  ``absolute=True`` sums
+    ``[n_voxels, 2]`` (start, count) into ``nb_list``; ``geom["nb_refine"]`` = r
+    > 1 puts the lists on the inner grid refined r times per axis (an
+    extension: lists within plateau + the refined half-diagonal find the same
+    pairs with fewer entries).  ``absolute=True`` sums
     |term| instead of term (magnitude scales for float32 tolerances).
     """
     dt = np.dtype(dtype)
@@ -310,8 +313,12 @@ def nb_energrad(pos, ltype, geom, nb_hdr, nb_list, rec, rtype, pair, mode="refer
     idx = np.nonzero(inn)[0]
     if len(idx) == 0:
         return E.reshape(shp), G.reshape(shp + (3,))
-    near = np.floor(v[idx] + dt.type(0.5)).astype(np.int64)
-    vox = (near[:, 0] * dim[1] + near[:, 1]) * dim[2] + near[:, 2]
+    # nearest list-grid point: the inner grid point itself, or -- for lists
+    # built on the inner grid refined r times per axis -- the refined point
+    r = int(geom.get("nb_refine", 1))
+    near = np.floor(v[idx] * r + dt.type(0.5)).astype(np.int64)
+    ndim = (dim - 1) * r + 1
+    vox = (near[:, 0] * ndim[1] + near[:, 1]) * ndim[2] + near[:, 2]
     start = nb_hdr[vox, 0].astype(np.int64)
     count = nb_hdr[vox, 1].astype(np.int64)
     tot = int(count.sum())

@@ -44,7 +44,7 @@ def test_potential_grid_builder_vs_oracle():
 def test_nbgrid_builder_vs_oracle():
     A, ff, geom, xyz, t = _small_receptor(seed=1)
     radius = 3.0 + np.sqrt(3) / 2 + 0.01
-    g = A.Grid.build(xyz, t, ff, geom, list_radius=radius, potentials=False)
+    g = A.Grid.build(xyz, t, ff, geom, list_radius=radius, potentials=False, nb_refine=1)
     _, _, hdr, lst = g.dense_host()
     ref_hdr, ref_lst = O.build_nbgrid(xyz, geom.as_dict(), radius)
     assert np.array_equal(hdr[:, 0], np.cumsum(hdr[:, 1]) - hdr[:, 1])  # CSR starts
@@ -58,6 +58,51 @@ def test_nbgrid_builder_vs_oracle():
             got[v, lst[s:s + n]] = True
         mismatch = got != (d <= radius)
         assert np.all(np.abs(d[mismatch] - radius) < 1e-4)
+
+
+@pytest.mark.parametrize("refine", [2, 4])
+def test_refined_list_grid_finds_the_same_pairs(refine):
+    """Lists on the inner grid refined 2x / 4x per axis (radius plateau + the
+    refined half-diagonal): the refined builder matches the oracle's lists on
+    the refined points, holds fewer entries per lookup, and the energies and
+    gradients equal those of the unrefined lists and the oracle's."""
+    A, ff, geom, xyz, t = _small_receptor(seed=2)
+    g1 = A.Grid.build(xyz, t, ff, geom, cutoff=6.0, nb_refine=1, keep_dense=True)
+    gr = A.Grid.build(xyz, t, ff, geom, cutoff=6.0, nb_refine=refine)
+    fine = geom.refined(refine)
+    radius = geom.plateau + fine.spacing * np.sqrt(3) / 2 + 1e-3
+    _, _, hdr, lst = gr.dense_host()
+    ref_hdr, ref_lst = O.build_nbgrid(xyz, fine.as_dict(), radius)
+    assert hdr.shape == ref_hdr.shape
+    pts = O.grid_points(fine.as_dict()).reshape(-1, 3)
+    for v in np.flatnonzero(hdr[:, 1] != ref_hdr[:, 1]):  # only float32 rounding at the radius
+        d = np.linalg.norm(pts[v] - xyz, axis=1)
+        got = set(lst[hdr[v, 0]:hdr[v, 0] + hdr[v, 1]].tolist())
+        want = set(np.flatnonzero(d <= radius).tolist())
+        assert all(abs(d[j] - radius) < 1e-4 for j in got ^ want)
+    rng = np.random.default_rng(5)
+    lig = rng.normal(size=(12, 3)) * 1.6
+    lt = rng.integers(0, geom.n_types, 12)
+    poses = np.concatenate([rng.uniform(-np.pi, np.pi, (96, 3)), rng.uniform(-4, 4, (96, 3))], 1)
+    P = torch.tensor(poses, dtype=torch.float32, device="cuda")
+    out = []
+    for g in (g1, gr):
+        wl = A.Workload([g], A.LigandSet([(lig, lt, lt)]), [A.Segment(0, 0, 96)], lanes_per_pose=32)
+        E, Gd, _ = A.energrad(wl, P)
+        _, _, _, st = A.minimise(wl, P, 1, stats=True)
+        out.append((E.cpu().numpy(), Gd.cpu().numpy(), st.cpu().numpy()))
+    (E1, G1, s1), (Er, Gr, sr) = out
+    scale = np.abs(E1) + 1.0
+    assert np.all(np.abs(Er - E1) <= 2e-5 * scale)
+    assert np.all(np.abs(Gr - G1) <= 2e-4 * (np.abs(G1) + 1.0))
+    assert sr[2] < s1[2]  # fewer list entries visited
+    inner, outer, h1, l1 = g1.dense_host()
+    Go = dict(geom=dict(geom.as_dict(), nb_refine=refine), inner=inner.astype(np.float64),
+              outer=outer.astype(np.float64), nb_hdr=hdr, nb_list=lst, rec=xyz, rtype=t,
+              pair=O.pair_table(ff.rc, ff.ac, ff.ivor, geom.plateau, True, ff.rcap2))
+    Eo, _ = O.energrad(poses.astype(np.float32).astype(np.float64), np.asarray(lig, np.float32).astype(np.float64),
+                       lt, lt, Go)
+    assert np.all(np.abs(Er - Eo) <= 2e-5 * (np.abs(Eo) + 1.0))
 
 
 def test_repack_bricks_exact():

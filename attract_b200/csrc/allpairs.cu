@@ -4,10 +4,13 @@
 // structure), with ATTRACT's --rcut as an optional distance cutoff.
 //
 // One block per pose (grid-stride over poses).  The receptor streams through
-// shared memory in tiles of ALLPAIRS_TILE beads; every thread holds one ligand
-// bead in registers and loops over the tile -- all threads read the same
-// receptor bead at the same time, a broadcast.  Per-thread sums (energy in
-// float, force, lever-arm products) are reduced over the block in double.
+// shared memory in tiles of ALLPAIRS_TILE beads.  A thread holds one ligand
+// bead in registers and takes a slice of every tile: with n ligand beads,
+// 256 / n threads share each bead (a small ligand still fills the block), so
+// a warp reads at most a few receptor beads at a time (broadcasts).  Per-thread
+// sums (energy in float, force, lever-arm products) are reduced over the block
+// in double; the torque is linear in the force, so partial forces of one bead
+// add up correctly.
 #include <math.h>
 
 #include "common.cuh"
@@ -87,9 +90,13 @@ __global__ void __launch_bounds__(ALLPAIRS_THREADS) allpairs_kernel(const __grid
     double acc[13];
 #pragma unroll
     for (int k = 0; k < 13; ++k) acc[k] = 0.0;
-    for (int i0 = 0; i0 < p.n_lig; i0 += ALLPAIRS_THREADS) {
-      const int i = i0 + threadIdx.x;
-      const bool live = i < p.n_lig;
+    // threads per bead (receptor slices) and this thread's bead / slice
+    const int nsl = p.n_lig < ALLPAIRS_THREADS ? ALLPAIRS_THREADS / p.n_lig : 1;
+    const int per = ALLPAIRS_THREADS / nsl;  // beads per pass
+    const int sl = (int)threadIdx.x / per;
+    for (int i0 = 0; i0 < p.n_lig; i0 += per) {
+      const int i = i0 + (int)threadIdx.x % per;
+      const bool live = i < p.n_lig && sl < nsl;
       float4 x = live ? __ldg(p.lig + i) : make_float4(0.f, 0.f, 0.f, 0.f);
       const int lt = live ? __float_as_int(x.w) : -1;
       const float X = fmaf(x.x, m[0], fmaf(x.y, m[3], fmaf(x.z, m[6], t[0])));
@@ -104,7 +111,7 @@ __global__ void __launch_bounds__(ALLPAIRS_THREADS) allpairs_kernel(const __grid
         for (int j = threadIdx.x; j < nt; j += ALLPAIRS_THREADS) s_rec[j] = __ldg(p.rec + j0 + j);
         __syncthreads();
         if (lok) {
-          for (int j = 0; j < nt; ++j) {
+          for (int j = sl; j < nt; j += nsl) {
             const float4 r = s_rec[j];
             const int rt = __float_as_int(r.w);
             const float dx = X - r.x, dy = Y - r.y, dz = Z - r.z;

@@ -256,12 +256,12 @@ def other_configs(args, device, shape):
             # list lengths seen by the starting poses' beads (the workload's "0-80 entries")
             xyz = np.asarray(cfg.ligands[0][0])
             X = np.einsum("bij,nj->bni", euler_to_Q(*poses_np[:20000, :3].T), xyz) + poses_np[:20000, None, 3:]
-            g = cfg.geom
+            g, ng, r = cfg.geom, grid.nb_geom, grid.nb_refine
             v = (X - np.asarray(g.origin)) / g.spacing
             inn = np.all((v >= 0) & (v < np.asarray(g.dim) - 1), axis=2)
-            near = np.floor(v + 0.5).astype(np.int64)
+            near = np.floor(v * r + 0.5).astype(np.int64)  # nearest list-grid point
             hdr = grid.nb_hdr.cpu().numpy().view(np.uint32)
-            vox = (near[..., 0] * g.dim[1] + near[..., 1]) * g.dim[2] + near[..., 2]
+            vox = (near[..., 0] * ng.dim[1] + near[..., 1]) * ng.dim[2] + near[..., 2]
             cnt = np.where(inn, hdr[np.clip(vox, 0, len(hdr) - 1), 1], 0)
             e["bead_fraction_with_lists"] = round(float((cnt > 0).mean()), 3)
             e["list_length_hist"] = np.bincount(np.minimum(cnt[cnt > 0], 80), minlength=81).tolist()

@@ -351,17 +351,11 @@ def serving_run(args, device):
 # --------------------------------------------------------------------------- ours
 def run_ours(args):
     import torch
-    import torch.distributed as dist
 
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(local)
-    device = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
+    from attract_b200 import replicas
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+    R = replicas.init("nccl")  # one process per GPU; replicas, no data-path collective
+    rank, world, local, device = R.rank, R.world, R.local, R.device
 
     import attract_b200 as A
     from attract_b200.autotune import autotune
@@ -395,8 +389,7 @@ def run_ours(args):
     clocks = Clocks(local)
     if rank == 0:
         clocks.start()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(R)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -405,12 +398,8 @@ def run_ours(args):
         plan.replay()
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(R, e0.elapsed_time(e1) / args.steps)
+    replicas.barrier(R)
     E = plan.scratch.energy
     status = plan.scratch.status
     n_bad = int((status != 0).sum().item())
@@ -425,8 +414,7 @@ def run_ours(args):
         host_E.copy_(plan.scratch.energy, non_blocking=True)
         host_P.copy_(plan.pose_out, non_blocking=True)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(R)
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record()
@@ -437,11 +425,7 @@ def run_ours(args):
         host_P.copy_(plan.pose_out, non_blocking=True)
     f1.record()
     torch.cuda.synchronize()
-    ms_e2e = f0.elapsed_time(f1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms_e2e], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = replicas.max_over_ranks(R, f0.elapsed_time(f1) / args.steps)
     clk = clocks.stop() if rank == 0 else None
 
     out = None
@@ -492,9 +476,7 @@ def run_ours(args):
             out["configs"] = other_configs(args, device, shape)
         if args.serve_seconds > 0:
             out["serving"] = serving_run(args, device)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(R)
     if rank == 0:
         print(json.dumps(out), flush=True)
 

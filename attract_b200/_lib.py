@@ -17,7 +17,11 @@ ATT_GRAD_ANALYTIC = 1
 ATT_FLAG_TRILINEAR_QUIRK = 1
 ATT_STATUS_NONFINITE_GRAD = 1
 ATT_STATUS_NONFINITE_ENERGY = 2
+ATT_STATUS_NONFINITE_POSE = 4
 ATT_MAX_GRIDS = 8
+ATT_KERR_COPY_TIMEOUT = 1
+ATT_KERR_BOUNDS = 2
+ATT_TEST_STALL_COPY_WAIT = 1
 ATT_NB_EMPTY = 65535
 
 
@@ -58,7 +62,7 @@ class AttAdamCfg(C.Structure):
 
 
 class AttLaunchCfg(C.Structure):
-    _fields_ = [("lanes_per_pose", C.c_int), ("block_threads", C.c_int), ("blocks", C.c_int), ("pad_", C.c_int)]
+    _fields_ = [("lanes_per_pose", C.c_int), ("block_threads", C.c_int), ("blocks", C.c_int), ("test_flags", C.c_int)]
 
 
 P = C.c_void_p

@@ -66,6 +66,7 @@ struct KParams {
   float lr_rot, lr_trans, b1, b2, eps;
   int step0;
   int rec_slot;          // bytes of a neighbour-record slot in shared memory (max over grids)
+  int test_flags;        // AttLaunchCfg.test_flags
   long long n_lig_beads;   // sizes for ATT_BOUNDS_CHECK builds
   long long n_dgrid_inner, n_dgrid_outer;
 };

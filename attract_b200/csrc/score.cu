@@ -87,7 +87,16 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-constexpr int WAIT_LIMIT = 1 << 22;  // try_wait polls before a bulk-copy wait is declared hung
+// A copy wait gives up after COPY_WAIT_NS of %globaltimer (read every 64
+// polls), or after WAIT_POLL_LIMIT polls, whichever comes first.
+constexpr unsigned long long COPY_WAIT_NS = 1000000000ull;  // 1 s
+constexpr unsigned WAIT_POLL_LIMIT = 1u << 26;
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // Loads with a fixed state space.  A list entry comes either from the
 // shared-memory record or from global memory; written as two distinct
@@ -308,6 +317,15 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
     }
     const float dLdE = (MODE == MODE_BWD && valid) ? __ldg(p.dLdE + b) : 0.f;
     int status = 0;
+    // a non-finite input pose is flagged (it places no bead on a grid)
+    if (MAT) {
+#pragma unroll
+      for (int k = 0; k < 12; ++k)
+        if (!isfinite(mat[k])) status |= ATT_STATUS_NONFINITE_POSE;
+    } else {
+      const unsigned team = (S == 32) ? 0xffffffffu : (((1u << S) - 1u) << lead);
+      if (__ballot_sync(0xffffffffu, valid && tl < 6 && !isfinite(my_x)) & team) status |= ATT_STATUS_NONFINITE_POSE;
+    }
     const int nsteps = (MODE == MODE_MIN) ? p.steps : 0;
     double bp1 = 1.0, bp2 = 1.0;  // beta1^t, beta2^t of the ADAM bias correction
     const int step0 = p.step0 + sg.step0;
@@ -461,7 +479,10 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
       }
       const unsigned warp_bytes = __reduce_add_sync(0xffffffffu, my_bytes);
       if (warp_bytes != 0) {
-        if (lane == 0) mbar_arrive_expect_tx(bar, warp_bytes);
+        // test hook (ATT_TEST_STALL_COPY_WAIT): the warp serving tile 0 expects
+        // 16 bytes that no copy delivers, so its bounded wait runs out
+        const unsigned stall = ((p.test_flags & ATT_TEST_STALL_COPY_WAIT) && tile == 0) ? 16u : 0u;
+        if (lane == 0) mbar_arrive_expect_tx(bar, warp_bytes + stall);
         __syncwarp();
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -475,8 +496,14 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
             held_v[k] = (int)nvox[k];
           }
         }
-        bool done = false;
-        for (int it = 0; it < WAIT_LIMIT && !done; ++it) done = mbar_try_wait(bar, parity);
+        bool done = mbar_try_wait(bar, parity);
+        if (!done) {
+          const unsigned long long t0 = globaltimer_ns();
+          for (unsigned it = 1; !done && it < WAIT_POLL_LIMIT; ++it) {
+            done = mbar_try_wait(bar, parity);
+            if (!done && (it & 63u) == 0u && globaltimer_ns() - t0 > COPY_WAIT_NS) break;
+          }
+        }
         if (!__all_sync(0xffffffffu, done)) {
           if (lane == 0) atomicOr(&g_kernel_error, ATT_KERR_COPY_TIMEOUT);
           return;  // a bulk copy never completed: report and leave (whole warp)
@@ -666,7 +693,7 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
               p.grad[(long long)b * 16 + k] = v;
             }
           }
-          if (tl == 0 && p.status != nullptr) p.status[b] = isfinite(etot) ? 0 : ATT_STATUS_NONFINITE_ENERGY;
+          if (tl == 0 && p.status != nullptr) p.status[b] = status | (isfinite(etot) ? 0 : ATT_STATUS_NONFINITE_ENERGY);
         }
         break;
       }

@@ -11,11 +11,16 @@ request does not depend on what it was batched with: per-pose arithmetic is
 independent of the other poses of a launch.
 
 Latency is wall-clock from ``submit`` to completion; ``stats()`` reports
-p50/p99 latency and sustained poses/s.
+p50/p99 latency and sustained poses/s.  Every finished request can be logged
+as one JSON line (``log_path``), and :meth:`DockingServer.snapshot` /
+:meth:`DockingServer.resume` checkpoint the unfinished ones between rounds:
+a request's pose and ADAM state are per pose and tiny, so a resumed request
+continues exactly where it stopped.  The phases of a round carry NVTX ranges.
 """
 from __future__ import annotations
 
 import bisect
+import json
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -27,6 +32,10 @@ from .engine import AdamOptions, EvalOptions, LaunchShape, Segment, Workload, mi
 from .ligand import LigandSet
 
 POSE_BYTES = 4 * (6 + 12 + 1 + 1)  # pose, ADAM state, energy, status
+
+
+def _lig_copy(lig):
+    return tuple(None if a is None else np.array(a) for a in lig)
 
 
 @dataclass
@@ -43,6 +52,8 @@ class Request:
     result_poses: np.ndarray | None = None
     result_energies: np.ndarray | None = None
     result_status: np.ndarray | None = None
+    adam0: np.ndarray | None = None   # [n, 12] ADAM moments to start from (a resumed request)
+    step0: int = 0                    # ADAM steps already taken (a resumed request)
 
     @property
     def n(self) -> int:
@@ -89,7 +100,7 @@ class PosePool:
 class DockingServer:
     def __init__(self, grids, steps: int = 200, round_steps: int = 25, max_inflight_poses: int = 1_000_000,
                  hbm_budget_bytes: float = 150e9, adam: AdamOptions | None = None, opts: EvalOptions | None = None,
-                 launch: LaunchShape | None = None, device=None):
+                 launch: LaunchShape | None = None, device=None, log_path: str | None = None):
         if steps % round_steps:
             raise ValueError("steps must be a multiple of round_steps")
         if len(grids) > 8:
@@ -121,6 +132,7 @@ class DockingServer:
         self.rounds = 0
         self.gpu_ms = 0.0
         self.t0 = time.perf_counter()
+        self.log = open(log_path, "a") if log_path else None
 
     # ------------------------------------------------------------------ API
     def submit(self, req: Request, now: float | None = None) -> Request:
@@ -161,10 +173,13 @@ class DockingServer:
             if s < 0:
                 break
             self.pending.popleft()
-            req.slot0, req.step, req.admitted = s, 0, now
+            req.slot0, req.step, req.admitted = s, req.step0, now
             self.pose[s:s + req.n].copy_(torch.from_numpy(np.ascontiguousarray(req.poses, np.float32)),
                                          non_blocking=True)
-            self.state[s:s + req.n].zero_()
+            if req.adam0 is None:
+                self.state[s:s + req.n].zero_()
+            else:
+                self.state[s:s + req.n].copy_(torch.from_numpy(np.ascontiguousarray(req.adam0, np.float32)))
             self.active.append(req)
 
     def _ligands(self):
@@ -177,9 +192,12 @@ class DockingServer:
     def round(self, now: float | None = None):
         """Admit what fits, advance every active request by round_steps, retire finished ones."""
         now = time.perf_counter() if now is None else now
+        torch.cuda.nvtx.range_push("serve.admit")
         self._admit(now)
+        torch.cuda.nvtx.range_pop()
         if not self.active:
             return
+        torch.cuda.nvtx.range_push("serve.round")
         # larger ligands first: they take the longest tiles
         order = sorted(range(len(self.active)), key=lambda i: -len(self.active[i].ligand[0]))
         segs = [Segment(self.active[i].receptor, i, self.active[i].n, self.active[i].step, self.active[i].slot0)
@@ -194,6 +212,8 @@ class DockingServer:
         e1.synchronize()
         self.gpu_ms += e0.elapsed_time(e1)
         self.rounds += 1
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.nvtx.range_push("serve.retire")
         t = time.perf_counter()
         still = []
         for r in self.active:
@@ -206,9 +226,52 @@ class DockingServer:
                 r.finished = t
                 self.pool.release(r.slot0, r.n)
                 self.done.append(r)
+                self._log(r)
             else:
                 still.append(r)
         self.active = still
+        torch.cuda.nvtx.range_pop()
+
+    def _log(self, r: Request):
+        if self.log is None:
+            return
+        E = r.result_energies
+        ok = np.isfinite(E) & (r.result_status == 0)
+        rec = {"rid": r.rid, "receptor": r.receptor, "poses": r.n, "beads": int(len(r.ligand[0])),
+               "arrival_s": r.arrival - self.t0, "admitted_s": r.admitted - self.t0,
+               "finished_s": r.finished - self.t0, "latency_s": r.latency, "queue_s": r.admitted - r.arrival,
+               "best_energy": float(E[ok].min()) if ok.any() else None,
+               "median_energy": float(np.median(E[ok])) if ok.any() else None,
+               "flagged_poses": int((~ok).sum())}
+        self.log.write(json.dumps(rec) + "\n")
+        self.log.flush()
+
+    # ------------------------------------------------------- checkpointing
+    def snapshot(self) -> dict:
+        """The unfinished requests, between rounds: per active request its
+        current poses, ADAM moments and step; pending requests as submitted.
+        Plain NumPy / Python values (``numpy.savez`` / pickle friendly)."""
+        torch.cuda.synchronize(self.device)
+        reqs = []
+        for r in self.active:
+            sl = slice(r.slot0, r.slot0 + r.n)
+            reqs.append(dict(receptor=r.receptor, ligand=_lig_copy(r.ligand),
+                             poses=self.pose[sl].cpu().numpy(), adam=self.state[sl].cpu().numpy(),
+                             step=r.step, rid=r.rid, arrival=r.arrival))
+        for r in self.pending:
+            reqs.append(dict(receptor=r.receptor, ligand=_lig_copy(r.ligand),
+                             poses=np.asarray(r.poses), adam=r.adam0, step=r.step0, rid=r.rid, arrival=r.arrival))
+        return {"steps": self.steps, "round_steps": self.round_steps, "requests": reqs}
+
+    @classmethod
+    def resume(cls, grids, snap: dict, **kw) -> "DockingServer":
+        """A server that continues the requests of ``snap`` (same receptors,
+        same step schedule); their results equal an uninterrupted run's."""
+        srv = cls(grids, steps=snap["steps"], round_steps=snap["round_steps"], **kw)
+        for q in snap["requests"]:
+            req = Request(q["receptor"], q["ligand"], q["poses"], adam0=q["adam"], step0=int(q["step"]))
+            srv.submit(req, now=q["arrival"])
+        return srv
 
 
 def replay(server: DockingServer, requests, duration: float | None = None, time_scale: float = 1.0,

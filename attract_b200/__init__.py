@@ -6,17 +6,19 @@ Public API
 ----------
 ForceField, GridGeom, Grid, LigandSet       -- inputs resident on the GPU
 Workload, Segment                           -- what one launch serves
-energrad, minimise, energrad_backward       -- the three kernels' entry points
+energrad, minimise, energrad_backward       -- the scoring kernels' entry points
+minimise_schema                             -- the reference's quaternion/adabelief protocol, fused
 MinimisePlan                                -- a graph-capturable batched minimisation
 EvalOptions, AdamOptions, LaunchShape       -- options
 """
 from ._lib import AttractError, load as load_library
 from .engine import (AdamOptions, EvalOptions, LaunchShape, MinimisePlan, MinimiseScratch, Segment, Workload,
-                     energrad, energrad_backward, minimise)
+                     energrad, energrad_backward, minimise, minimise_schema)
 from .forcefield import ForceField
 from .grid import Grid, GridGeom
 from .ligand import LigandSet
 
 __all__ = ["AttractError", "load_library", "AdamOptions", "EvalOptions", "LaunchShape", "MinimisePlan",
-           "MinimiseScratch", "Segment", "Workload", "energrad", "energrad_backward", "minimise", "ForceField",
+           "MinimiseScratch", "Segment", "Workload", "energrad", "energrad_backward", "minimise", "minimise_schema",
+           "ForceField",
            "Grid", "GridGeom", "LigandSet"]

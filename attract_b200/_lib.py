@@ -61,6 +61,15 @@ class AttAdamCfg(C.Structure):
                 ("beta2", C.c_float), ("eps", C.c_float), ("step0", C.c_int)]
 
 
+ATT_MAX_STAGES = 8
+
+
+class AttSchemaCfg(C.Structure):
+    _fields_ = [("eval", AttEvalCfg), ("n_stages", C.c_int), ("epochs", C.c_int * ATT_MAX_STAGES),
+                ("lr", C.c_float * ATT_MAX_STAGES), ("gravity", C.c_int * ATT_MAX_STAGES), ("beta1", C.c_float),
+                ("beta2", C.c_float), ("eps", C.c_float), ("eps_root", C.c_float)]
+
+
 class AttLaunchCfg(C.Structure):
     _fields_ = [("lanes_per_pose", C.c_int), ("block_threads", C.c_int), ("blocks", C.c_int), ("test_flags", C.c_int)]
 
@@ -91,6 +100,8 @@ SIGNATURES = {
     "att_nbgrid_pack_records": (I, [P, P, LL, I, P, P]),
     "att_kernel_debug_info": (I, [C.POINTER(C.c_ulonglong), I, P]),
     "att_allpairs_energy": (I, [P, I, P, I, P, I, I, P, I, I, F, P, P, P]),
+    "att_minimise_schema": (I, [C.POINTER(AttGrid), I, C.POINTER(AttLigands), P, I, P, I, P, P, P,
+                                C.POINTER(AttSchemaCfg), P, P, P, C.POINTER(AttLaunchCfg), P]),
 }
 
 _lib = None

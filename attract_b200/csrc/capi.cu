@@ -299,6 +299,57 @@ extern "C" int att_minimise(const AttGrid* grids, int n_grids, const AttLigands*
   return ATT_OK;
 }
 
+extern "C" int att_minimise_schema(const AttGrid* grids, int n_grids, const AttLigands* ligs,
+                                   const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
+                                   const float* pose_in_dev, float* pose_out_dev, const int* pose_lig_dev,
+                                   const AttSchemaCfg* cfg, float* energy_dev, int* status_dev,
+                                   int* work_counter_dev, const AttLaunchCfg* launch, void* stream) {
+  REQUIRE(cfg != nullptr, "schema cfg is NULL");
+  KParams p;
+  int S = 8, K = 1, threads = 128;
+  int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, pose_in_dev,
+                       pose_lig_dev, &cfg->eval, launch, &S, &K, &threads);
+  if (rc) return rc;
+  REQUIRE(cfg->n_stages >= 1 && cfg->n_stages <= ATT_MAX_STAGES, "n_stages = %d (1..%d)", cfg->n_stages,
+          ATT_MAX_STAGES);
+  int total = 0;
+  for (int i = 0; i < cfg->n_stages; ++i) {
+    REQUIRE(cfg->epochs[i] >= 0, "stage %d: epochs < 0", i);
+    total += cfg->epochs[i];
+  }
+  REQUIRE(total >= 1, "the schema has no epochs");
+  REQUIRE(cfg->beta1 >= 0.f && cfg->beta1 < 1.f && cfg->beta2 >= 0.f && cfg->beta2 < 1.f,
+          "beta1/beta2 must be in [0, 1)");
+  REQUIRE(pose_out_dev != nullptr || n_tiles == 0, "pose_out is NULL");
+  REQUIRE(energy_dev != nullptr || n_tiles == 0, "energy output is NULL");
+  REQUIRE(work_counter_dev != nullptr, "work counter is NULL");
+  p.pose_out = pose_out_dev;
+  p.energy = energy_dev;
+  p.status = status_dev;
+  p.counter = work_counter_dev;
+  p.steps = total;
+  p.b1 = cfg->beta1;
+  p.b2 = cfg->beta2;
+  p.eps = cfg->eps;
+  p.eps_root = cfg->eps_root;
+  p.qs_n = cfg->n_stages;
+  for (int i = 0; i < ATT_MAX_STAGES; ++i) {
+    p.qs_epochs[i] = i < cfg->n_stages ? cfg->epochs[i] : 0;
+    p.qs_lr[i] = i < cfg->n_stages ? cfg->lr[i] : 0.f;
+    p.qs_grav[i] = i < cfg->n_stages ? cfg->gravity[i] : 0;
+  }
+  if (n_tiles == 0) return ATT_OK;
+  int blocks = 0;
+  rc = persistent_blocks(MODE_QUAT, S, K, threads, p.rec_slot, launch, n_tiles, &blocks);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(work_counter_dev, 0, sizeof(int), st);
+  if (e != cudaSuccess) return cuda_fail(e, "att_minimise_schema counter reset");
+  e = launch_score(p, MODE_QUAT, S, K, blocks, threads, st);
+  if (e != cudaSuccess) return cuda_fail(e, "att_minimise_schema launch");
+  return ATT_OK;
+}
+
 extern "C" int att_energrad_backward(const AttGrid* grids, int n_grids, const AttLigands* ligs,
                                      const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
                                      const float* pose_dev, const int* pose_lig_dev, const AttEvalCfg* cfg,

@@ -37,7 +37,7 @@ struct __align__(16) KGrid {
   const float4* pair;             // [n_ltypes][n_rtypes][2] float4
 };
 
-enum Mode { MODE_EVAL = 0, MODE_EVAL_MAT = 1, MODE_MIN = 2, MODE_BWD = 3 };
+enum Mode { MODE_EVAL = 0, MODE_EVAL_MAT = 1, MODE_MIN = 2, MODE_BWD = 3, MODE_QUAT = 4 };
 
 struct KParams {
   KGrid grid[ATT_MAX_GRIDS];
@@ -67,6 +67,11 @@ struct KParams {
   int step0;
   int rec_slot;          // bytes of a neighbour-record slot in shared memory (max over grids)
   int test_flags;        // AttLaunchCfg.test_flags
+  int qs_n;               // MODE_QUAT: SCHEMA stages, epochs / learning rate / gravity on-off per stage
+  int qs_epochs[ATT_MAX_STAGES];
+  float qs_lr[ATT_MAX_STAGES];
+  int qs_grav[ATT_MAX_STAGES];
+  float eps_root;
   long long n_lig_beads;   // sizes for ATT_BOUNDS_CHECK builds
   long long n_dgrid_inner, n_dgrid_outer;
 };

@@ -211,6 +211,8 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
   constexpr int U = 2;           // pair slots in flight per lane
   constexpr int PB = PAIRS_PER_BEAD * NB;  // pair-buffer window of one team
   constexpr bool MAT = (MODE == MODE_EVAL_MAT);
+  constexpr bool QUAT = (MODE == MODE_QUAT);   // quaternion + adabelief SCHEMA protocol
+  constexpr bool ACC9 = MAT || QUAT;           // accumulate dE/dmat (ligand-frame lever arms)
   extern __shared__ __align__(128) unsigned char smem_raw[];
 
   const int lane = threadIdx.x & 31;
@@ -308,6 +310,8 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
 #pragma unroll
       for (int k = 0; k < 12; ++k)
         mat[k] = valid ? __ldg(p.pose_in + (long long)b * 16 + (k / 3) * 4 + (k % 3)) : 0.f;
+    } else if (QUAT) {  // lanes 0..6: qx, qy, qz, qw (scalar last), tx, ty, tz; moments start at 0
+      if (valid && tl < 7) my_x = __ldg(p.pose_in + (long long)b * 8 + tl);
     } else if (valid && tl < 6) {
       my_x = __ldg(p.pose_in + (long long)b * 6 + tl);
       if (MODE == MODE_MIN && p.adam != nullptr) {
@@ -324,9 +328,41 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
         if (!isfinite(mat[k])) status |= ATT_STATUS_NONFINITE_POSE;
     } else {
       const unsigned team = (S == 32) ? 0xffffffffu : (((1u << S) - 1u) << lead);
-      if (__ballot_sync(0xffffffffu, valid && tl < 6 && !isfinite(my_x)) & team) status |= ATT_STATUS_NONFINITE_POSE;
+      if (__ballot_sync(0xffffffffu, valid && tl < (QUAT ? 7 : 6) && !isfinite(my_x)) & team)
+        status |= ATT_STATUS_NONFINITE_POSE;
     }
-    const int nsteps = (MODE == MODE_MIN) ? p.steps : 0;
+    // quaternion protocol: normalise the input quaternion (Rotation.from_quat),
+    // then track the SCHEMA stage, its epoch count and bias-correction powers
+    auto normalise_quat = [&]() {
+      const float a0 = __shfl_sync(0xffffffffu, my_x, lead + 0), a1 = __shfl_sync(0xffffffffu, my_x, lead + 1);
+      const float a2 = __shfl_sync(0xffffffffu, my_x, lead + 2), a3 = __shfl_sync(0xffffffffu, my_x, lead + 3);
+      const float n = sqrtf(fmaf(a0, a0, fmaf(a1, a1, fmaf(a2, a2, a3 * a3))));
+      if (tl < 4) my_x = my_x / n;
+    };
+    int stage = 0, k_stage = 0;  // current stage and epochs taken in it
+    int st_epochs = 0, st_grav = 0;
+    float st_lr = 0.f;
+    float last_E = 0.f;          // energy of the latest evaluation (reported, test5.py:465)
+    // the values of stage `st` (static parameter indices only: the tables stay
+    // in the constant bank, never indexed dynamically in parameter space)
+    auto load_stage = [&](int st) {
+      st_epochs = 0;
+      st_lr = 0.f;
+      st_grav = 0;
+#pragma unroll
+      for (int i = 0; i < ATT_MAX_STAGES; ++i)
+        if (i == st) {
+          st_epochs = p.qs_epochs[i];
+          st_lr = p.qs_lr[i];
+          st_grav = p.qs_grav[i];
+        }
+    };
+    if (QUAT) {
+      normalise_quat();
+      load_stage(stage);
+      while (stage < p.qs_n && st_epochs == 0) load_stage(++stage);
+    }
+    const int nsteps = (MODE == MODE_MIN || QUAT) ? p.steps : 0;  // QUAT: total epochs
     double bp1 = 1.0, bp2 = 1.0;  // beta1^t, beta2^t of the ADAM bias correction
     const int step0 = p.step0 + sg.step0;
     if (MODE == MODE_MIN && step0 > 0) {
@@ -338,11 +374,32 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
       // ---------------- pose -> rotation Q (column form) and translation t
       float q00, q01, q02, q10, q11, q12, q20, q21, q22, tx, ty, tz;
       float sphi = 0.f, cphi = 1.f, spsi = 0.f, cpsi = 1.f;
+      float qx = 0.f, qy = 0.f, qz = 0.f, qw = 1.f;  // QUAT: the pose's quaternion
       if (MAT) {
         q00 = mat[0]; q10 = mat[1]; q20 = mat[2];
         q01 = mat[3]; q11 = mat[4]; q21 = mat[5];
         q02 = mat[6]; q12 = mat[7]; q22 = mat[8];
         tx = mat[9]; ty = mat[10]; tz = mat[11];
+      } else if (QUAT) {
+        // the row-vector matrix of Rotation.as_matrix (homogeneous quaternion
+        // form, test5.py:413); column-form Q is its transpose
+        qx = __shfl_sync(0xffffffffu, my_x, lead + 0);
+        qy = __shfl_sync(0xffffffffu, my_x, lead + 1);
+        qz = __shfl_sync(0xffffffffu, my_x, lead + 2);
+        qw = __shfl_sync(0xffffffffu, my_x, lead + 3);
+        const float x = qx, y = qy, z = qz, w = qw;
+        tx = __shfl_sync(0xffffffffu, my_x, lead + 4);
+        ty = __shfl_sync(0xffffffffu, my_x, lead + 5);
+        tz = __shfl_sync(0xffffffffu, my_x, lead + 6);
+        q00 = x * x - y * y - z * z + w * w;  // M00
+        q11 = -x * x + y * y - z * z + w * w;  // M11
+        q22 = -x * x - y * y + z * z + w * w;  // M22
+        q10 = 2.f * (x * y - z * w);           // M01
+        q20 = 2.f * (x * z + y * w);           // M02
+        q01 = 2.f * (x * y + z * w);           // M10
+        q21 = 2.f * (y * z - x * w);           // M12
+        q02 = 2.f * (x * z - y * w);           // M20
+        q12 = 2.f * (y * z + x * w);           // M21
       } else {
         // team lanes 0..2 hold the three angles: one sincosf per lane, then
         // broadcast (one sincos instruction stream per warp instead of three)
@@ -370,9 +427,9 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
       }
 
       float acc_e = 0.f, acc_gx = 0.f, acc_gy = 0.f, acc_gz = 0.f;
-      float acc_t[MAT ? 9 : 3];
+      float acc_t[ACC9 ? 9 : 3];
 #pragma unroll
-      for (int k = 0; k < (MAT ? 9 : 3); ++k) acc_t[k] = 0.f;
+      for (int k = 0; k < (ACC9 ? 9 : 3); ++k) acc_t[k] = 0.f;
 
       for (int chunk = 0; chunk < nchunk; ++chunk) {
       const int c0 = chunk * NB;
@@ -448,7 +505,7 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
           bp.x = X; bp.y = Y; bp.z = Z; bp.lt = lt;
           bpos[tbase + i] = bp;
           BeadArm ba;
-          if (MAT) { ba.x = lx[k]; ba.y = ly[k]; ba.z = lz[k]; }
+          if (ACC9) { ba.x = lx[k]; ba.y = ly[k]; ba.z = lz[k]; }
           else { ba.x = rx; ba.y = ry; ba.z = rz; }
           ba.pad = 0.f;
           barm[tbase + i] = ba;
@@ -588,12 +645,12 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
               float px, py, pz;
               pair_term_masked(p, G, bp, rr[m], acc_e, px, py, pz);
               BeadArm ba;  // lever arm: Q x = X - t (the 4x4 form needs the ligand-frame x)
-              if (MAT) ba = barm[bi];
+              if (ACC9) ba = barm[bi];
               else { ba.x = bp.x - tx; ba.y = bp.y - ty; ba.z = bp.z - tz; }
               acc_gx += px;
               acc_gy += py;
               acc_gz += pz;
-              if (MAT) {
+              if (ACC9) {
                 acc_t[0] = fmaf(ba.x, px, acc_t[0]); acc_t[1] = fmaf(ba.x, py, acc_t[1]); acc_t[2] = fmaf(ba.x, pz, acc_t[2]);
                 acc_t[3] = fmaf(ba.y, px, acc_t[3]); acc_t[4] = fmaf(ba.y, py, acc_t[4]); acc_t[5] = fmaf(ba.y, pz, acc_t[5]);
                 acc_t[6] = fmaf(ba.z, px, acc_t[6]); acc_t[7] = fmaf(ba.z, py, acc_t[7]); acc_t[8] = fmaf(ba.z, pz, acc_t[8]);
@@ -653,7 +710,7 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
           acc_gx += gbx;
           acc_gy += gby;
           acc_gz += gbz;
-          if (MAT) {
+          if (ACC9) {
             acc_t[0] = fmaf(ba.x, gbx, acc_t[0]); acc_t[1] = fmaf(ba.x, gby, acc_t[1]); acc_t[2] = fmaf(ba.x, gbz, acc_t[2]);
             acc_t[3] = fmaf(ba.y, gbx, acc_t[3]); acc_t[4] = fmaf(ba.y, gby, acc_t[4]); acc_t[5] = fmaf(ba.y, gbz, acc_t[5]);
             acc_t[6] = fmaf(ba.z, gbx, acc_t[6]); acc_t[7] = fmaf(ba.z, gby, acc_t[7]); acc_t[8] = fmaf(ba.z, gbz, acc_t[8]);
@@ -675,7 +732,56 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
       acc_gy = team_sum<S>(acc_gy);
       acc_gz = team_sum<S>(acc_gz);
 #pragma unroll
-      for (int k = 0; k < (MAT ? 9 : 3); ++k) acc_t[k] = team_sum<S>(acc_t[k]);
+      for (int k = 0; k < (ACC9 ? 9 : 3); ++k) acc_t[k] = team_sum<S>(acc_t[k]);
+
+      if constexpr (QUAT) {
+        // ---- SCHEMA protocol step (test5.py:450-458): energy and gradient
+        // with this stage's gravity, dE/dq from dE/dM through the quaternion
+        // form, optax.adabelief update on lanes 0..6, renormalised quaternion
+        const float grav = st_grav ? p.gravity : 0.f;
+        last_E = acc_e + grav * (tx * tx + ty * ty + tz * tz);
+        const float G00 = acc_t[0], G01 = acc_t[1], G02 = acc_t[2];
+        const float G10 = acc_t[3], G11 = acc_t[4], G12 = acc_t[5];
+        const float G20 = acc_t[6], G21 = acc_t[7], G22 = acc_t[8];
+        const float x = qx, y = qy, z = qz, w = qw;
+        const float gqx = 2.f * (G00 * x + G01 * y + G02 * z + G10 * y - G11 * x - G12 * w + G20 * z + G21 * w - G22 * x);
+        const float gqy = 2.f * (-G00 * y + G01 * x + G02 * w + G10 * x + G11 * y + G12 * z - G20 * w + G21 * z - G22 * y);
+        const float gqz = 2.f * (-G00 * z - G01 * w + G02 * x + G10 * w - G11 * z + G12 * y + G20 * x + G21 * y + G22 * z);
+        const float gqw = 2.f * (G00 * w - G01 * z + G02 * y + G10 * z + G11 * w - G12 * x - G20 * y + G21 * x + G22 * w);
+        const float gtx = acc_gx + 2.f * grav * tx, gty = acc_gy + 2.f * grav * ty, gtz = acc_gz + 2.f * grav * tz;
+        float gk = gqx;
+        gk = (tl == 1) ? gqy : gk;
+        gk = (tl == 2) ? gqz : gk;
+        gk = (tl == 3) ? gqw : gk;
+        gk = (tl == 4) ? gtx : gk;
+        gk = (tl == 5) ? gty : gk;
+        gk = (tl == 6) ? gtz : gk;
+        const bool ok = isfinite(gqx) & isfinite(gqy) & isfinite(gqz) & isfinite(gqw) & isfinite(gtx) &
+                        isfinite(gty) & isfinite(gtz);
+        ++k_stage;
+        bp1 *= (double)p.b1;
+        bp2 *= (double)p.b2;
+        if (!ok) {
+          status |= ATT_STATUS_NONFINITE_GRAD;
+        } else if (tl < 7) {
+          const float err = gk - my_m;  // against the previous first moment (optax scale_by_belief)
+          my_m = fmaf(p.b1, my_m, (1.f - p.b1) * gk);
+          my_v = fmaf(p.b2, my_v, (1.f - p.b2) * err * err) + p.eps_root;
+          const float mh = my_m / (float)(1.0 - bp1);
+          const float vh = my_v / (float)(1.0 - bp2);
+          my_x -= st_lr * mh / (sqrtf(vh) + p.eps);
+        }
+        normalise_quat();  // Rotation.from_quat(rotations.as_quat())
+        if (k_stage >= st_epochs) {  // next stage: a fresh optimiser state
+          load_stage(++stage);
+          while (stage < p.qs_n && st_epochs == 0) load_stage(++stage);
+          k_stage = 0;
+          my_m = my_v = 0.f;
+          bp1 = bp2 = 1.0;
+        }
+        if (s + 1 >= nsteps) break;
+        continue;
+      }
 
       const float etot = acc_e + p.gravity * (tx * tx + ty * ty + tz * tz);
       if (MAT) {
@@ -741,6 +847,11 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
       }
     }
 
+    if (QUAT && valid) {
+      if (tl < 7) p.pose_out[(long long)b * 8 + tl] = my_x;
+      if (tl == 0) p.energy[b] = last_E;
+      if (!isfinite(last_E)) status |= ATT_STATUS_NONFINITE_ENERGY;
+    }
     if (MODE == MODE_MIN && valid && tl < 6) {
       p.pose_out[(long long)b * 6 + tl] = my_x;
       if (p.adam != nullptr) {
@@ -748,7 +859,8 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
         p.adam[(long long)b * 12 + 6 + tl] = my_v;
       }
     }
-    if ((MODE == MODE_MIN || MODE == MODE_EVAL) && valid && tl == 0 && p.status != nullptr) p.status[b] = status;
+    if ((MODE == MODE_MIN || MODE == MODE_EVAL || QUAT) && valid && tl == 0 && p.status != nullptr)
+      p.status[b] = status;
 
     if (p.counter != nullptr) {
       int t0 = 0;
@@ -792,6 +904,7 @@ static const void* kernel_of(int mode, int S, int K) {
     case MODE_EVAL_MAT: return KernelTable<MODE_EVAL_MAT>::get(S, K);
     case MODE_MIN: return KernelTable<MODE_MIN>::get(S, K);
     case MODE_BWD: return KernelTable<MODE_BWD>::get(S, K);
+    case MODE_QUAT: return KernelTable<MODE_QUAT>::get(S, K);
   }
   return nullptr;
 }

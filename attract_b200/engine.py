@@ -239,6 +239,45 @@ def minimise(wl: Workload, poses: torch.Tensor, steps: int, adam: AdamOptions | 
     return pose_out, scratch.energy, scratch.status, st
 
 
+def minimise_schema(wl: Workload, poses: torch.Tensor, schema, opts: EvalOptions | None = None, *,
+                    gravity_weight: float = 0.1, betas=(0.9, 0.999), eps: float = 1e-16, eps_root: float = 1e-16,
+                    pose_out: torch.Tensor | None = None, pose_lig: torch.Tensor | None = None,
+                    launch: LaunchShape | None = None, stream=None, scratch=None):
+    """The reference's SCHEMA protocol (quaternion poses, optax.adabelief per
+    stage, gravity per stage) in one persistent launch: ``poses`` is ``[B, 8]``
+    (qx, qy, qz, qw, tx, ty, tz, unused); ``schema`` a sequence of (epochs,
+    learning rate, gravity on) stages.  Returns ``(pose_out [B, 8], E of the
+    last evaluation [B], status [B])``."""
+    opts = opts or EvalOptions()
+    launch = launch or LaunchShape(lanes_per_pose=wl.lanes)
+    if launch.lanes_per_pose != wl.lanes:
+        raise ValueError("launch.lanes_per_pose differs from the workload's tiling")
+    wl.check_poses(poses, 8)
+    stages = [tuple(st) for st in schema]
+    if not 1 <= len(stages) <= _lib.ATT_MAX_STAGES:
+        raise ValueError(f"1..{_lib.ATT_MAX_STAGES} schema stages")
+    if pose_out is None:
+        pose_out = torch.empty_like(poses)
+    if pose_lig is not None:
+        _check_pose_lig(wl, pose_lig)
+    if scratch is None:
+        scratch = MinimiseScratch(wl.n_poses, wl.device)
+    cfg = _lib.AttSchemaCfg()
+    cfg.eval = EvalOptions(opts.grad_mode, opts.quirk, gravity_weight).to_c(0)
+    cfg.n_stages = len(stages)
+    for i, (ep, lr, grav) in enumerate(stages):
+        cfg.epochs[i], cfg.lr[i], cfg.gravity[i] = int(ep), float(lr), int(bool(grav))
+    cfg.beta1, cfg.beta2, cfg.eps, cfg.eps_root = float(betas[0]), float(betas[1]), float(eps), float(eps_root)
+    lc = launch.to_c()
+    rc = _lib.load().att_minimise_schema(wl.c_grids, len(wl.grids), C.byref(wl.c_ligs), _lib.ptr(wl.segs),
+                                         len(wl.segments), _lib.ptr(wl.seg_tile), wl.n_tiles, _lib.ptr(poses),
+                                         _lib.ptr(pose_out), _lib.ptr(pose_lig), C.byref(cfg),
+                                         _lib.ptr(scratch.energy), _lib.ptr(scratch.status),
+                                         _lib.ptr(scratch.counter), C.byref(lc), _stream(stream))
+    _lib.check(rc, "att_minimise_schema")
+    return pose_out, scratch.energy, scratch.status
+
+
 class MinimiseScratch:
     """Output and work-queue buffers of one minimisation launch."""
 

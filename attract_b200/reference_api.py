@@ -250,20 +250,39 @@ class AdaBelief:
 
 
 def minimise_schema(rotations, translations, coor_rec, rec_atomtypes, coor_lig, lig_atomtypes, conformers,
-                    lig_atomtype_pos, ff, grid, schema=SCHEMA):
+                    lig_atomtype_pos, ff, grid, schema=SCHEMA, fused=True):
     """The reference's minimisation protocol (test5.py:445-463): per SCHEMA
     stage ``(epochs, learning_rate, gravity)`` a fresh adabelief state over
     (quaternion, translation); each epoch evaluates energies and gradients,
     applies the update and renormalises the quaternion
     (``Rotation.from_quat(rotations.as_quat())``).  Returns ``(quaternions,
     translations, energies)`` where, as in the reference, the energies are
-    those of the last evaluation (test5.py:465)."""
-    check_call(rotations, translations, conformers)
+    those of the last evaluation (test5.py:465).  ``fused`` runs the whole
+    protocol in one persistent kernel launch (att_minimise_schema); otherwise
+    one energy/gradient launch per epoch with the optimiser in torch ops, the
+    reference's own dispatch pattern."""
+    B, conf = check_call(rotations, translations, conformers)
     prep = _prepare(coor_rec, rec_atomtypes, coor_lig, lig_atomtypes, lig_atomtype_pos, ff, grid)
     q, _ = _rotations(rotations, prep.grid.device)
     if q is None:
         raise AssertionError("minimise_schema takes quaternion rotations")
     t = torch.as_tensor(_np(translations), dtype=torch.float32, device=prep.grid.device)
+    if fused:
+        from .engine import minimise_schema as _fused
+
+        if conf is None:
+            if prep.n_conf != 1:
+                raise AssertionError("a conformer library needs conformer indices")
+        elif B and conf.max() >= prep.n_conf:
+            raise AssertionError("conformer index outside the conformer library")
+        qt = torch.zeros((B, 8), dtype=torch.float32, device=prep.grid.device)
+        qt[:, :4] = q
+        qt[:, 4:7] = t
+        pose_lig = (torch.as_tensor(conf.astype(np.int32), device=prep.grid.device)
+                    if prep.n_conf > 1 and conf is not None else None)
+        out, E, _ = _fused(prep.workload(B), qt, schema, EvalOptions(grad_mode="reference", quirk=True),
+                           gravity_weight=GRAVITY, pose_lig=pose_lig, launch=LaunchShape(32))
+        return out[:, :4].clone(), out[:, 4:7].clone(), E.clone()
     E = None
     for epochs, lr, gravity in schema:
         opt = AdaBelief([q, t], lr)

@@ -13,6 +13,8 @@
  *                        (and the 4x4-matrix form of test1.py:361-366,409-412)
  *   att_minimise         the batch/epoch optimiser loop, test5.py:436-467
  *                        (optax.adam form of test4.py:440-455)
+ *   att_minimise_schema  the same loop with test5's own protocol: quaternion
+ *                        poses, optax.adabelief, the SCHEMA stages, test5.py:14-23,445-467
  *   att_energrad_backward  reverse mode of test5.py:429, extended to the grid
  *                        values (no counterpart: JAX never differentiates the grid)
  *   att_grid_repack      the dense grid arrays of read_grid2.py:92-155
@@ -143,6 +145,20 @@ typedef struct AttAdamCfg {
   int step0;        /* steps already taken by the given adam_state (bias correction) */
 } AttAdamCfg;
 
+/* The minimisation protocol of test5.py:14-23,436-467: stages of (epochs,
+   learning rate, gravity on/off), each with a fresh optax.adabelief state over
+   the (quaternion, translation) pose. */
+#define ATT_MAX_STAGES 8
+typedef struct AttSchemaCfg {
+  AttEvalCfg eval;          /* grad_mode, flags; gravity = weight of |t|^2 in stages with gravity on
+                               (test5.py:419: 0.1); pose_format ignored */
+  int n_stages;             /* 1..ATT_MAX_STAGES */
+  int epochs[ATT_MAX_STAGES];
+  float lr[ATT_MAX_STAGES];
+  int gravity[ATT_MAX_STAGES];
+  float beta1, beta2, eps, eps_root;  /* optax.adabelief defaults: 0.9, 0.999, 1e-16, 1e-16 */
+} AttSchemaCfg;
+
 /* Launch shape; zeros pick the defaults / autotuned values. */
 typedef struct AttLaunchCfg {
   int lanes_per_pose;   /* 8, 16 or 32 (poses per warp = 32 / lanes_per_pose) */
@@ -194,6 +210,22 @@ int att_minimise(const AttGrid* grids, int n_grids, const AttLigands* ligs,
                  float* adam_state_dev, const AttAdamCfg* cfg, int steps,
                  float* energy_dev, int* status_dev, int* work_counter_dev,
                  unsigned long long* stats_dev, const AttLaunchCfg* launch, void* stream);
+
+/* The whole SCHEMA protocol (test5.py:445-467) as one persistent launch:
+   pose_in_dev / pose_out_dev [B][8] = qx, qy, qz, qw (scalar last), tx, ty,
+   tz, unused (may alias).  The input quaternion is normalised
+   (Rotation.from_quat); every epoch evaluates E and dE/d(q, t) -- dE/dq through
+   Rotation.as_matrix's homogeneous quaternion form -- applies the adabelief
+   update (prediction error against the previous first moment, as optax's
+   scale_by_belief) and renormalises the quaternion.  energy_dev [B] receives
+   the energy of the last evaluation, before the last update, as the reference
+   reports it (test5.py:465).  A step with a non-finite gradient is skipped and
+   flagged in status_dev.  work_counter_dev: one int of scratch. */
+int att_minimise_schema(const AttGrid* grids, int n_grids, const AttLigands* ligs,
+                        const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
+                        const float* pose_in_dev, float* pose_out_dev, const int* pose_lig_dev,
+                        const AttSchemaCfg* cfg, float* energy_dev, int* status_dev, int* work_counter_dev,
+                        const AttLaunchCfg* launch, void* stream);
 
 /* Adjoint of att_energrad for L = sum_b dL_dE[b] * E[b]: dL/dpose [B][6] and the
    scatter-add of dL/d(grid energy values) into dgrid_inner_dev / dgrid_outer_dev,

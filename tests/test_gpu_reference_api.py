@@ -126,3 +126,27 @@ def test_schema_minimisation_reproduces_the_oracle_ranking():
     assert rho > 0.98, rho
     close = np.abs(Eg - Eo) <= 1e-3 * np.abs(Eo) + 1e-2
     assert close.mean() >= 0.9, close.mean()
+
+
+def test_fused_schema_kernel_matches_the_per_epoch_path():
+    """att_minimise_schema (the whole protocol in one launch) against the
+    per-epoch path (one energy/gradient launch per epoch, adabelief in torch
+    ops): the same float32 arithmetic in a different order, so the
+    trajectories agree closely; every stage boundary (fresh optimiser state,
+    gravity switched off) is crossed."""
+    from attract_b200.reference_api import minimise_schema
+
+    c, q, t, confs, conformers, args, es, gs = _setup(seed=62, n_poses=64)
+    Eo0, _, _ = O.energrad_quat(q, t, confs, conformers, c["gt"], c["lt"], c["G"])
+    keep = Eo0 < 1e3
+    q, t = q[keep], t[keep]
+    args = dict(args, conformers=conformers[keep])
+    schema = ((3, 0.5, True), (0, 1.0, True), (4, 0.1, False), (3, 0.02, False))
+    qf, tf, Ef = minimise_schema(q, t, **args, schema=schema, fused=True)
+    qh, th, Eh = minimise_schema(q, t, **args, schema=schema, fused=False)
+    qf, tf, Ef = qf.cpu().numpy(), tf.cpu().numpy(), Ef.cpu().numpy()
+    qh, th, Eh = qh.cpu().numpy(), th.cpu().numpy(), Eh.cpu().numpy()
+    assert np.allclose(np.linalg.norm(qf, axis=1), 1.0, atol=1e-5)
+    same = (np.abs(tf - th).max(1) < 1e-3) & (np.minimum(np.abs(qf - qh), np.abs(qf + qh)).max(1) < 1e-3)
+    assert same.mean() >= 0.9, same.mean()
+    assert np.all(np.abs(Ef - Eh)[same] <= 1e-3 * np.abs(Eh[same]) + 1e-2)

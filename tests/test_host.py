@@ -42,7 +42,8 @@ def test_ctypes_layouts_match_the_c_header(tmp_path):
     from attract_b200 import _lib
 
     src = tmp_path / "probe.c"
-    structs = ["AttGridGeom", "AttGrid", "AttLigands", "AttSegment", "AttEvalCfg", "AttAdamCfg", "AttLaunchCfg"]
+    structs = ["AttGridGeom", "AttGrid", "AttLigands", "AttSegment", "AttEvalCfg", "AttAdamCfg", "AttLaunchCfg",
+               "AttSchemaCfg"]
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "attract_b200.h"', "int main(void){"]
     for s in structs:
         lines.append(f'printf("{s} %zu\\n", sizeof({s}));')

@@ -298,6 +298,43 @@ def other_configs(args, device, shape):
                        "value": round(wl.n_poses / ms_ap * 1e3, 1), "unit": "poses/s",
                        "pairs_per_s": round(n_pairs / ms_ap * 1e3, 1)}
     del ap
+    # the reference's own protocol (test5.py: 375 adabelief epochs over quaternion poses, SCHEMA
+    # stages with gravity) through the drop-in call surface, on 200 000 poses (test5's batch)
+    from attract_b200 import reference_api as R
+    from attract_b200.poses import random_in_ball
+
+    rng = np.random.default_rng(3)
+    nq = max(1000, int(200_000 * args.scale))
+    quats = rng.normal(size=(nq, 4))  # uniform rotations: normalised 4-D Gaussians
+    quats = (quats / np.linalg.norm(quats, axis=1, keepdims=True)).astype(np.float32)
+    trans = random_in_ball(nq, 30.0, rng).astype(np.float32)
+    rec_t = np.asarray(cfg.rec_type)
+    kw = dict(coor_rec=cfg.rec_xyz, rec_atomtypes=rec_t, coor_lig=lig[0], lig_atomtypes=lig[2], conformers=None,
+              lig_atomtype_pos=lig[1], ff=cfg.ff, grid=grid)
+    R.minimise_schema(quats[:1000], trans[:1000], **kw, schema=((2, 0.1, True),))  # warm
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    _, _, Ef = R.minimise_schema(quats, trans, **kw, fused=True)
+    t1.record()
+    torch.cuda.synchronize()
+    ms_f = t0.elapsed_time(t1)
+    t0.record()
+    _, _, Eh = R.minimise_schema(quats, trans, **kw, fused=False)
+    t1.record()
+    torch.cuda.synchronize()
+    ms_h = t0.elapsed_time(t1)
+    res["schema"] = {"workload": f"test5 protocol: SCHEMA 375 adabelief epochs, quaternion poses, {nq} poses, "
+                                 "config-1 receptor (2500 beads), 24-bead ligand",
+                     "fused": {"ms": round(ms_f, 1), "value": round(nq / ms_f * 1e3, 1), "unit": "poses/s"},
+                     "per_epoch_launches": {"ms": round(ms_h, 1), "value": round(nq / ms_h * 1e3, 1),
+                                            "unit": "poses/s",
+                                            "note": "one att_energrad launch per epoch, adabelief in torch ops"},
+                     "fused_vs_per_epoch": round(ms_h / ms_f, 2),
+                     "median_energy_fused": float(np.median(Ef.cpu().numpy())),
+                     "median_energy_per_epoch": float(np.median(Eh.cpu().numpy())),
+                     "reference_published": "~3 M structures/hour = 833 poses/s (test5.py:6-7, unspecified "
+                                            "hardware; context only)"}
     res["config3"] = {"workload": "differentiation: config-1 receptor, 24-bead ligand, 65536 poses, summed energy, "
                                   "backward to poses and grid energies (analytic mode)",
                       "poses": wl.n_poses, "ms_forward_backward": round(ms, 3),

@@ -267,3 +267,24 @@ def test_zz_kernel_error_word_is_clear():
 
     torch.cuda.synchronize()
     assert _lib.kernel_status(clear=True) == 0
+
+
+def test_record_size_does_not_change_results():
+    """Neighbour records of 32 B (13 entries inline, the rest read from the CSR
+    tail) and of 128 B (everything inline here) hold the same lists in the
+    same order: identical results, bit for bit."""
+    A = _A()
+    c = small_case(seed=96, n_poses=48)
+    res = []
+    for rb in (32, 128):
+        grid = to_device_grid(c)
+        grid._pack_records(rec_bytes=rb)
+        grid._att = None
+        if rb == 32:
+            assert int((grid.nb_hdr[:, 1] > 13).sum()) > 0
+        wl = A.Workload([grid], A.LigandSet([(c["lig"], c["gt"], c["lt"])]), [A.Segment(0, 0, 48)],
+                        lanes_per_pose=32)
+        P = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+        out, E, _, _ = A.minimise(wl, P, 6)
+        res.append((out.cpu().numpy(), E.cpu().numpy()))
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])

@@ -4,9 +4,12 @@ A :class:`Grid` holds, on one CUDA device:
 
 * ``bricks``  -- the potential grids (inner + outer, every ligand type) repacked
   so that the 8 trilinear corners of a voxel are one contiguous, 128-byte
-  aligned run of float4 ``(E, Fx, Fy, Fz)``: one coalesced 128-B read per bead;
+  aligned run of float4 ``(E, Fx, Fy, Fz)``: one 128-B bulk copy per bead,
+  made only when the bead enters another cell;
 * ``nb_hdr`` / ``nb_list`` -- the neighbour grid as CSR: ``{start, count}`` per
-  inner grid point and uint16 receptor indices (65535 = empty slot);
+  list-grid point (the inner grid, or the inner grid refined ``nb_refine``
+  times) and uint16 receptor indices (65535 = empty slot), with the fixed-size
+  records ``nb_rec`` the kernels copy;
 * ``rec`` -- receptor beads ``x, y, z, type`` (float4, type as int32 bits);
 * ``pair`` -- the per-pair parameter table for this grid's plateau.
 

@@ -362,11 +362,11 @@ def serving_run(args, device):
     pool = np.concatenate([random_rotations(400_000, rng), random_in_ball(400_000, 30.0, rng)], 1).astype(np.float32)
     draw = lambda n: pool[(o := int(rng.integers(0, len(pool) - n))):o + n]
     desc = ("4 resident receptors (1500/3000/4500/6000 beads), ligands U{5..60} beads, poses lognormal(median "
-            "10000, sigma 1.0) clipped to [1000, 200000], 200 ADAM steps in rounds of 25")
+            "10000, sigma 1.0) clipped to [1000, 200000], 200 ADAM steps in rounds of 25; each round one launch "
+            "per launch shape (lanes per pose 8/16/32 and beads per lane by ligand size)")
 
     def one(rate):
-        srv = DockingServer(grids, steps=200, round_steps=25, max_inflight_poses=600_000, hbm_budget_bytes=150e9,
-                            launch=A.LaunchShape(32))
+        srv = DockingServer(grids, steps=200, round_steps=25, max_inflight_poses=600_000, hbm_budget_bytes=150e9)
         reqs = synth.serving_requests(int(args.serve_seconds * rate * 1.5) + 10, seed=0, rate=rate)
         st = replay(srv, reqs, duration=args.serve_seconds, pose_source=draw)
         offered = sum(q["n_poses"] for q in reqs if q["t"] <= args.serve_seconds) / args.serve_seconds

@@ -52,6 +52,33 @@ def test_result_alone_equals_result_in_the_mix(grids):
     assert st["requests"] == 5 and st["p99_s"] >= st["p50_s"] > 0
 
 
+@pytest.mark.parametrize("concurrent", [True, False])
+def test_alone_equals_mix_across_launch_shapes(grids, concurrent):
+    """Requests of different launch shapes (lanes per pose picked per ligand
+    size, 1 and 2 beads per lane) in the same rounds: each result equals the
+    request's result alone, bit for bit, whether the shape groups run on
+    their own streams or one after another."""
+    lanes_for = lambda n: 8 if n <= 8 else (16 if n <= 16 else 32)
+    specs = [(30, 0, 6, 50), (31, 1, 60, 45), (32, 2, 14, 70), (33, 1, 27, 40), (34, 0, 40, 33)]
+    alone = {}
+    for sp in specs:
+        srv = _server(grids, steps=30, round_steps=10, max_inflight_poses=5000, lanes_for=lanes_for)
+        r = srv.submit(_req(*sp))
+        srv.run_until_idle()
+        alone[sp] = r
+    mix = _server(grids, steps=30, round_steps=10, max_inflight_poses=5000, lanes_for=lanes_for,
+                  concurrent=concurrent)
+    got = {sp: mix.submit(_req(*sp)) for sp in specs[:3]}
+    mix.round()
+    got.update({sp: mix.submit(_req(*sp)) for sp in specs[3:]})
+    mix.run_until_idle()
+    assert {mix.shape_of(sp[2]) for sp in specs} == {(8, 1), (32, 2), (16, 1), (32, 1)}
+    assert mix.stats()["launches"] > mix.stats()["rounds"]
+    for sp in specs:
+        assert np.array_equal(alone[sp].result_poses, got[sp].result_poses), sp
+        assert np.array_equal(alone[sp].result_energies, got[sp].result_energies), sp
+
+
 def test_rounds_equal_one_launch(grids):
     import attract_b200 as A
 

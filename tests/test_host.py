@@ -148,3 +148,17 @@ def test_workload_tiling_on_cpu():
         Workload([g], L, [Segment(0, 2, 1)])
     with pytest.raises(ValueError):
         LigandSet([(np.zeros((2, 3)), [0, 70000], None)], device="cpu")
+
+
+def test_serving_launch_shapes():
+    """A request's launch shape follows its own ligand size: beads per lane
+    as the kernel picks them (next power of two, at most 4)."""
+    from attract_b200.serve import launch_shape
+
+    assert launch_shape(1, 32) == (32, 1) and launch_shape(32, 32) == (32, 1)
+    assert launch_shape(33, 32) == (32, 2) and launch_shape(64, 32) == (32, 2)
+    assert launch_shape(65, 32) == (32, 4) and launch_shape(500, 32) == (32, 4)
+    assert launch_shape(9, 8) == (8, 2) and launch_shape(17, 8) == (8, 4) and launch_shape(16, 16) == (16, 1)
+    for bad in ((10, 12), (0, 32)):
+        with pytest.raises(ValueError):
+            launch_shape(*bad)

@@ -250,6 +250,7 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
   // statistics (MODE_MIN): bead evaluations with a brick, list lookups, list
   // entries, brick copies, record copies
   unsigned c_grid = 0, c_look = 0, c_ent = 0, c_cpb = 0, c_cpr = 0;
+  const bool want_stats = p.stats != nullptr;
 
   int tile;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -527,7 +528,7 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
         need_b[k] = use[k] && (int)bidx[k] != held_b[k];
         need_v[k] = nvox[k] >= 0 && (int)nvox[k] != held_v[k];
         my_bytes += (need_b[k] ? 128u : 0u) + (need_v[k] ? (unsigned)G.nb_rec_bytes : 0u);
-        if (MODE == MODE_MIN) {
+        if (MODE == MODE_MIN && want_stats) {
           c_grid += use[k] ? 1u : 0u;
           c_look += nvox[k] >= 0 ? 1u : 0u;
           c_cpb += need_b[k] ? 1u : 0u;
@@ -585,7 +586,7 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
           ck[k] = (nvox[k] >= 0) ? lds_u16(rk + 4) : 0u;
           my_total += ck[k];
         }
-        if (MODE == MODE_MIN) c_ent += my_total;
+        if (MODE == MODE_MIN && want_stats) c_ent += my_total;
         unsigned incl = my_total;  // inclusive scan over the team's lanes
 #pragma unroll
         for (int off = 1; off < S; off <<= 1) {
@@ -672,14 +673,21 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
           const float4* br = bricks + (size_t)(tbase + tl + k * S) * 8;
           float eb = 0.f, gbx = 0.f, gby = 0.f, gbz = 0.f;
           const float sc = gscale[k];
+          // Step q reads corner c = q ^ r (r = tl & 7): the 8 lanes of a bank
+          // phase read 8 different 16-B bank groups of their 128-B bricks, and
+          // the corner's x/y/z offsets are q's static bits flipped by r's, so
+          // each weight is a compile-time choice between two per-bead values.
+          const int r = tl & 7;
+          const int rx = (r >> 2) & 1, ry = (r >> 1) & 1, rz = r & 1;
+          const float wx0 = rx ? fx[k] : 1.f - fx[k], wx1 = rx ? 1.f - fx[k] : fx[k];  // q bit 0 / 1
+          const float wy0 = ry ? fy[k] : 1.f - fy[k], wy1 = ry ? 1.f - fy[k] : fy[k];
+          const float wz0 = rz ? fz[k] : 1.f - fz[k], wz1 = rz ? 1.f - fz[k] : fz[k];
+          const float sx0 = rx ? 1.f : -1.f, sy0 = ry ? 1.f : -1.f, sz0 = rz ? 1.f : -1.f;  // d(weight)/d(frac)
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
-            const int c = (q + tl) & 7;  // rotated: 8 lanes hit 8 different bank groups
+            const int c = q ^ r;
             const float4 v = br[c];
-            const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
-            const float wx = cx ? fx[k] : 1.f - fx[k];
-            const float wy = cy ? fy[k] : 1.f - fy[k];
-            const float wz = cz ? fz[k] : 1.f - fz[k];
+            const float wx = (q & 4) ? wx1 : wx0, wy = (q & 2) ? wy1 : wy0, wz = (q & 1) ? wz1 : wz0;
             const float w = wx * wy * wz;
             eb = fmaf(w, v.x, eb);
             if (p.grad_mode == ATT_GRAD_REFERENCE) {
@@ -688,11 +696,13 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
               gbz = fmaf(-w, v.w, gbz);
             } else {
               const float ce = v.x * sc;
-              gbx = fmaf(ce, (cx ? 1.f : -1.f) * wy * wz, gbx);
-              gby = fmaf(ce, wx * (cy ? 1.f : -1.f) * wz, gby);
-              gbz = fmaf(ce, wx * wy * (cz ? 1.f : -1.f), gbz);
+              const float sx = (q & 4) ? -sx0 : sx0, sy = (q & 2) ? -sy0 : sy0, sz = (q & 1) ? -sz0 : sz0;
+              gbx = fmaf(ce, sx * wy * wz, gbx);
+              gby = fmaf(ce, wx * sy * wz, gby);
+              gbz = fmaf(ce, wx * wy * sz, gbz);
             }
             if (MODE == MODE_BWD) {
+              const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
               float* dg = outer_k[k] ? p.dgrid_outer : p.dgrid_inner;
               if (dg != nullptr) {
                 const int nx = outer_k[k] ? G.dx2 : G.dx;

@@ -1,7 +1,7 @@
 """Run the batched minimiser on a synthetic workload a few times (for profilers).
 
     python -m attract_b200.profile_case [--config 1] [--scale 0.05] [--types 32]
-        [--launches 3] [--lanes 32] [--threads 64] [--steps N] [--refine 2]
+        [--launches 3] [--lanes 32] [--threads 64] [--steps N] [--refine 4]
 
 Builds the workload (grid build, neighbour lists, bricks), then launches the
 persistent minimisation kernel ``--launches`` times and prints the mean time of
@@ -26,7 +26,7 @@ def main():
     ap.add_argument("--lanes", type=int, default=32)
     ap.add_argument("--threads", type=int, default=64)
     ap.add_argument("--steps", type=int, default=-1)
-    ap.add_argument("--refine", type=int, default=2, help="neighbour-list grid refinement (1, 2 or 4)")
+    ap.add_argument("--refine", type=int, default=4, help="neighbour-list grid refinement (1, 2 or 4)")
     a = ap.parse_args()
 
     import attract_b200 as A

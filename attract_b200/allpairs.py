@@ -13,7 +13,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .engine import _stream
+from .engine import _stream, _used_on
 from .forcefield import ForceField
 from .grid import _dev, pack_receptor
 
@@ -50,6 +50,7 @@ class AllPairs:
                                              _lib.ptr(self.pair), self.ff.n_rtypes, self.ff.n_ltypes,
                                              float(rcut or 0.0), _lib.ptr(E), _lib.ptr(G), _stream(stream))
         _lib.check(rc, "att_allpairs_energy")
+        _used_on(stream, p2, E, G)
         if G is not None and mat:
             G = G.view(B, 4, 4)
         return E, G

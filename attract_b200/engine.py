@@ -89,6 +89,21 @@ def _stream(stream):
     return int(stream)
 
 
+def _used_on(stream, *tensors):
+    """A launch on ``stream`` (not the current stream) reads or writes
+    ``tensors``, which the caching allocator assigned to the current stream:
+    record the use, so that their memory is not handed out again before that
+    stream's work is done."""
+    if stream is None:
+        return
+    s = stream if isinstance(stream, torch.cuda.Stream) else torch.cuda.ExternalStream(int(stream))
+    if s.cuda_stream == torch.cuda.current_stream().cuda_stream:
+        return
+    for t in tensors:
+        if t is not None:
+            t.record_stream(s)
+
+
 class Workload:
     """Device tables for launches over ``segments`` (see module docstring)."""
 
@@ -189,6 +204,7 @@ def energrad(wl: Workload, poses: torch.Tensor, opts: EvalOptions | None = None,
                                   _lib.ptr(pose_lig), C.byref(cfg), _lib.ptr(E), _lib.ptr(G), _lib.ptr(S),
                                   C.byref(lc), _stream(stream))
     _lib.check(rc, "att_energrad")
+    _used_on(stream, wl.segs, wl.seg_tile, p2, pose_lig, E, G, S)
     if G is not None and mat:
         G = G.view(B, 4, 4)
     return E, G, S
@@ -236,6 +252,8 @@ def minimise(wl: Workload, poses: torch.Tensor, steps: int, adam: AdamOptions | 
                                   int(steps), _lib.ptr(scratch.energy), _lib.ptr(scratch.status),
                                   _lib.ptr(scratch.counter), _lib.ptr(st), C.byref(lc), _stream(stream))
     _lib.check(rc, "att_minimise")
+    _used_on(stream, wl.segs, wl.seg_tile, poses, pose_out, pose_lig, adam_state, scratch.energy, scratch.status,
+             scratch.counter, st)
     return pose_out, scratch.energy, scratch.status, st
 
 
@@ -275,6 +293,7 @@ def minimise_schema(wl: Workload, poses: torch.Tensor, schema, opts: EvalOptions
                                          _lib.ptr(scratch.energy), _lib.ptr(scratch.status),
                                          _lib.ptr(scratch.counter), C.byref(lc), _stream(stream))
     _lib.check(rc, "att_minimise_schema")
+    _used_on(stream, wl.segs, wl.seg_tile, poses, pose_out, pose_lig, scratch.energy, scratch.status, scratch.counter)
     return pose_out, scratch.energy, scratch.status
 
 
@@ -306,6 +325,7 @@ def energrad_backward(wl: Workload, poses: torch.Tensor, dL_dE: torch.Tensor, op
                                            _lib.ptr(dgrid_inner), _lib.ptr(dgrid_outer), C.byref(lc),
                                            _stream(stream))
     _lib.check(rc, "att_energrad_backward")
+    _used_on(stream, wl.segs, wl.seg_tile, poses, pose_lig, dL_dE, out, dgrid_inner, dgrid_outer)
     return out
 
 

@@ -260,6 +260,11 @@ class DockingServer:
         main = torch.cuda.current_stream(self.device)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(main)
+        # The groups' segment tables are allocated on the current stream and
+        # read by kernels on the groups' streams: they stay referenced until
+        # the round has synchronised, so the caching allocator cannot hand
+        # their memory to another group's tables while a kernel reads them.
+        tables = []
         # the largest beads-per-lane groups first: their tiles take longest
         for shape in sorted(groups, key=lambda sh: (-sh[1], -sh[0])):
             # within a launch, larger ligands first
@@ -267,6 +272,7 @@ class DockingServer:
             lig_key, ligs, counter, stream = self._group(shape, reqs)
             segs = [Segment(r.receptor, i, r.n, r.step, r.slot0) for i, r in enumerate(reqs)]
             wl = Workload(self.grids, ligs, segs, shape[0], self.device, n_poses=self.capacity)
+            tables.append(wl)
             scratch = _GroupScratch(self.scratch, counter)
             launch = LaunchShape(shape[0], self.launch.block_threads, self.launch.blocks, self.launch.test_flags)
             if stream is not None:
@@ -279,6 +285,7 @@ class DockingServer:
             self.launches += 1
         e1.record(main)
         e1.synchronize()
+        del tables
         self.gpu_ms += e0.elapsed_time(e1)
         self.rounds += 1
         torch.cuda.nvtx.range_pop()

@@ -217,6 +217,28 @@ def test_graph_capture_replay_matches_direct():
     assert torch.equal(o1, out2) and torch.equal(e1, E2)
 
 
+def test_side_stream_launches_equal_current_stream():
+    """energrad / minimise / backward on a caller-given stream (a torch Stream
+    or a raw handle) equal the current-stream results; the temporaries they
+    allocate are recorded on that stream, so repeated launches whose buffers
+    are dropped right away stay correct."""
+    A, c, wl = _minimise_case(seed=18, n_poses=48)
+    P = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+    E0, G0, _ = A.energrad(wl, P)
+    o0, m0, _, _ = A.minimise(wl, P, 6)
+    b0 = A.energrad_backward(wl, P, torch.ones(48, device="cuda"))
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    for s in (side, side.cuda_stream):
+        for _ in range(3):  # every buffer of the earlier iterations is already released
+            E1, G1, _ = A.energrad(wl, P, stream=s)
+            o1, m1, _, _ = A.minimise(wl, P, 6, stream=s)
+            b1 = A.energrad_backward(wl, P, torch.ones(48, device="cuda"), stream=s)
+        side.synchronize()
+        assert torch.equal(E0, E1) and torch.equal(G0, G1)
+        assert torch.equal(o0, o1) and torch.equal(m0, m1) and torch.equal(b0, b1)
+
+
 def test_minimise_stats_counts():
     A, c, wl = _minimise_case(seed=18, n_poses=32)
     P = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")

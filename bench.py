@@ -472,6 +472,8 @@ def run_ours(args):
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
             os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
         peak = float(peaks.get("hbm_gbs", 6650.0))
+        peak_source = ("measured hbm_gbs (MEASURED_PEAKS.json)" if "hbm_gbs" in peaks
+                       else "fallback 6650 GB/s (no MEASURED_PEAKS.json on this machine)")
         achieved = alg_bytes / (ms / 1e3) / 1e9
         bead_evals = int(stats[0])
         traffic = traffic_from_profile(bead_evals)
@@ -491,7 +493,7 @@ def run_ours(args):
             "gpu_launches": args.steps * 1,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "algorithmic_bytes_per_launch": alg_bytes, "peak_source": "measured hbm_gbs",
+                         "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_source,
                          "counts": {"brick_reads": int(stats[0]), "list_lookups": int(stats[1]),
                                     "list_entries": int(stats[2])}},
             "clocks": clk,

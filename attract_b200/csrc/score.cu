@@ -146,15 +146,18 @@ __device__ __noinline__ void bounds_report(int code, long long a, long long b) {
 #endif
 
 // shared memory of one warp: per bead slot a 128-B brick, a neighbour-record
-// slot of rec_slot bytes and two 16-B bead records; the pair buffers of the
+// slot of rec_slot bytes, a 16-B moved-bead record and, in the modes that
+// accumulate dE/dmat, a 16-B ligand-frame record; the pair buffers of the
 // warp's teams (PAIRS_PER_BEAD u32 words per bead slot, plus S words of
 // padding per team so that teams start in different banks); the mbarrier
 constexpr int PAIRS_PER_BEAD = 8;
 __host__ __device__ inline int rec_stride(int rec_slot) { return rec_slot ? rec_slot + 16 : 0; }
 __host__ __device__ inline size_t pair_buffer_bytes(int K) { return (size_t)32 * (PAIRS_PER_BEAD * K + 1) * 4; }
-__host__ __device__ inline size_t warp_smem_bytes(int K, int rec_slot) {
-  return (size_t)32 * K * (128 + rec_stride(rec_slot) + sizeof(BeadPos) + sizeof(BeadArm)) + pair_buffer_bytes(K) +
-         16;
+// (the bead arms are held only by the modes that accumulate dE/dmat; the
+// others take the lever arm from the bead record)
+__host__ __device__ inline size_t warp_smem_bytes(int K, int rec_slot, bool arms = true) {
+  return (size_t)32 * K * (128 + rec_stride(rec_slot) + sizeof(BeadPos) + (arms ? sizeof(BeadArm) : 0)) +
+         pair_buffer_bytes(K) + 16;
 }
 
 template <int S>
@@ -221,13 +224,14 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
   const int tl = lane % S;
   const int lead = slot * S;
   const int RS = rec_stride(p.rec_slot);
-  unsigned char* wsm = smem_raw + (size_t)warp * warp_smem_bytes(K, p.rec_slot);
+  unsigned char* wsm = smem_raw + (size_t)warp * warp_smem_bytes(K, p.rec_slot, ACC9);
   float4* bricks = reinterpret_cast<float4*>(wsm);                          // [32K][8]
   unsigned char* nrec = wsm + 32 * K * 128;                                 // [32K][RS]
   BeadPos* bpos = reinterpret_cast<BeadPos*>(nrec + 32 * K * RS);
-  BeadArm* barm = reinterpret_cast<BeadArm*>(nrec + 32 * K * (RS + 16));
-  uint32_t* pbuf = reinterpret_cast<uint32_t*>(nrec + 32 * K * (RS + 32));
-  uint64_t* bar = reinterpret_cast<uint64_t*>(nrec + 32 * K * (RS + 32) + pair_buffer_bytes(K));
+  BeadArm* barm = reinterpret_cast<BeadArm*>(nrec + 32 * K * (RS + 16));  // ACC9 modes only
+  constexpr int ARM_BYTES = ACC9 ? 16 : 0;
+  uint32_t* pbuf = reinterpret_cast<uint32_t*>(nrec + 32 * K * (RS + 16 + ARM_BYTES));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(nrec + 32 * K * (RS + 16 + ARM_BYTES) + pair_buffer_bytes(K));
   const int tbase = slot * NB;  // this team's first bead record
   uint32_t* pb = pbuf + slot * (PB + S);  // this team's pair buffer
 
@@ -505,11 +509,12 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
           BeadPos bp;
           bp.x = X; bp.y = Y; bp.z = Z; bp.lt = lt;
           bpos[tbase + i] = bp;
-          BeadArm ba;
-          if (ACC9) { ba.x = lx[k]; ba.y = ly[k]; ba.z = lz[k]; }
-          else { ba.x = rx; ba.y = ry; ba.z = rz; }
-          ba.pad = 0.f;
-          barm[tbase + i] = ba;
+          if (ACC9) {
+            BeadArm ba;
+            ba.x = lx[k]; ba.y = ly[k]; ba.z = lz[k];
+            ba.pad = 0.f;
+            barm[tbase + i] = ba;
+          }
         }
       }
       // One bulk copy per brick and per neighbour record whose slot does not
@@ -715,7 +720,13 @@ __global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kern
               }
             }
           }
-          const BeadArm ba = barm[tbase + tl + k * S];
+          BeadArm ba;  // lever arm: Q x = X - t, as in the pair term (ACC9: ligand-frame x)
+          if (ACC9) {
+            ba = barm[tbase + tl + k * S];
+          } else {
+            const BeadPos bq = bpos[tbase + tl + k * S];
+            ba.x = bq.x - tx; ba.y = bq.y - ty; ba.z = bq.z - tz;
+          }
           acc_e += eb;
           acc_gx += gbx;
           acc_gy += gby;
@@ -930,10 +941,17 @@ size_t score_smem_bytes(int K, int threads, int rec_slot) {
   return warp_smem_bytes(K, rec_slot) * (size_t)(threads / 32);
 }
 
+// the shared memory of one block of `mode` (without bead arms unless the mode
+// accumulates dE/dmat)
+static size_t mode_smem_bytes(int mode, int K, int threads, int rec_slot) {
+  const bool arms = mode == MODE_EVAL_MAT || mode == MODE_QUAT;
+  return warp_smem_bytes(K, rec_slot, arms) * (size_t)(threads / 32);
+}
+
 cudaError_t launch_score(const KParams& p, int mode, int S, int K, int blocks, int threads, cudaStream_t st) {
   const void* k = kernel_of(mode, S, K);
   if (k == nullptr) return cudaErrorInvalidValue;
-  const size_t smem = score_smem_bytes(K, threads, p.rec_slot);
+  const size_t smem = mode_smem_bytes(mode, K, threads, p.rec_slot);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   void* args[] = {const_cast<KParams*>(&p)};
@@ -966,7 +984,7 @@ cudaError_t kernel_debug_info(unsigned long long* out3, int clear, cudaStream_t 
 cudaError_t occupancy_blocks(int mode, int S, int K, int threads, int rec_slot, int* blocks_per_sm) {
   const void* k = kernel_of(mode, S, K);
   if (k == nullptr) return cudaErrorInvalidValue;
-  const size_t smem = score_smem_bytes(K, threads, rec_slot);
+  const size_t smem = mode_smem_bytes(mode, K, threads, rec_slot);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k, threads, smem);

@@ -111,6 +111,12 @@ def lanes_by_size(n_beads: int) -> int:
     return 8 if n_beads <= 8 else 16 if n_beads <= 16 else 32
 
 
+def launch_order(r: "Request"):
+    """Sort key of the requests within one launch: larger ligands first (their
+    tiles take longest, so they do not end up in the launch's tail)."""
+    return -len(r.ligand[0])
+
+
 def launch_shape(n_beads: int, lanes: int) -> tuple[int, int]:
     """(lanes per pose, beads per lane) for a ligand of ``n_beads`` beads: the
     beads per lane the kernel picks for it (the next power of two of
@@ -267,8 +273,7 @@ class DockingServer:
         tables = []
         # the largest beads-per-lane groups first: their tiles take longest
         for shape in sorted(groups, key=lambda sh: (-sh[1], -sh[0])):
-            # within a launch, larger ligands first
-            reqs = sorted(groups[shape], key=lambda r: -len(r.ligand[0]))
+            reqs = sorted(groups[shape], key=launch_order)
             lig_key, ligs, counter, stream = self._group(shape, reqs)
             segs = [Segment(r.receptor, i, r.n, r.step, r.slot0) for i, r in enumerate(reqs)]
             wl = Workload(self.grids, ligs, segs, shape[0], self.device, n_poses=self.capacity)

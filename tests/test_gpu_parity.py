@@ -76,6 +76,26 @@ def test_energrad_branches_ivor_nocap_gravity():
     assert np.all(dG <= 5 * np.abs(G32 - Go) + 1e-4 * gs[:, None] + 1e-3)
 
 
+@pytest.mark.parametrize("n_beads,lanes", [(30, 32), (60, 32), (60, 16), (60, 8)])
+def test_dense_lists_many_pair_windows(n_beads, lanes):
+    """A dense receptor (lists of ~100 entries, mostly in the CSR overflow)
+    and ligands of up to 60 beads: each team's pairs fill its pair buffer many
+    times over (at 1, 2, 4 and 8 beads per lane), and the result still matches
+    the oracle."""
+    A = _engine()
+    c = small_case(seed=31, n_rec=400, n_lig_beads=n_beads, n_poses=40)
+    grid = to_device_grid(c)
+    wl = _wl(A, grid, c["lig"], c["gt"], c["lt"], len(c["poses"]), lanes)
+    poses = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+    E, G, S = A.energrad(wl, poses)
+    Eo, Go = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], c["G"])
+    es, gs = oracle_scales(c, c["poses"])
+    _check(E.cpu().numpy(), G.cpu().numpy(), Eo, Go, es, gs)
+    # the case does reach many windows: entries per pose far above a team's buffer
+    hdr = c["G"]["nb_hdr"]
+    assert hdr[:, 1].max() > 64
+
+
 @pytest.mark.parametrize("what", ["grid_only", "nb_only", "inner_only"])
 def test_energrad_partial_grids(what):
     A = _engine()

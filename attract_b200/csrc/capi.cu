@@ -155,6 +155,11 @@ static int make_kgrid(const AttGrid* a, int gi, KGrid* k) {
   }
   k->rec = reinterpret_cast<const float4*>(a->rec);
   k->pair = reinterpret_cast<const float4*>(a->pair);
+  // the scoring kernels remember which brick and which list point a bead's
+  // shared-memory slots hold as 32-bit indices
+  REQUIRE(k->n_bricks <= 2147483647LL, "grid %d: %lld bricks; at most 2^31 - 1", gi, k->n_bricks);
+  REQUIRE(a->nb_hdr == nullptr || k->n_vox <= 2147483647LL, "grid %d: %lld list points; at most 2^31 - 1", gi,
+          k->n_vox);
   return ATT_OK;
 }
 

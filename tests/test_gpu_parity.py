@@ -179,6 +179,15 @@ def test_host_validation_errors():
     wl = _wl(A, grid, c["lig"], c["gt"], c["lt"], 4)
     with pytest.raises(ValueError):
         A.energrad(wl, torch.zeros((5, 6), dtype=torch.float32, device="cuda"))
+    # a list grid of more than 2^31 - 1 points is rejected before any launch
+    # (the kernels hold list-point indices in 32 bits)
+    g = wl.c_grids[0]
+    g.bricks, g.n_inner_bricks, g.n_outer_bricks = None, 0, 0
+    for k in range(3):
+        g.geom.dim[k] = 700
+    g.nb_refine = 4
+    with pytest.raises(A.AttractError, match="list points"):
+        A.energrad(wl, torch.zeros((4, 6), dtype=torch.float32, device="cuda"))
 
 
 # --------------------------------------------------------------------------- golden

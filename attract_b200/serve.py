@@ -88,7 +88,13 @@ class PosePool:
         return -1
 
     def release(self, s: int, n: int):
+        """Return [s, s + n) to the pool; a range outside the pool or
+        overlapping free space (a double release) raises ValueError."""
+        if n <= 0 or s < 0 or s + n > self.capacity:
+            raise ValueError(f"release of [{s}, {s + n}) outside the pool [0, {self.capacity})")
         i = bisect.bisect_left(self.free, (s, 0))
+        if (i > 0 and self.free[i - 1][0] + self.free[i - 1][1] > s) or (i < len(self.free) and self.free[i][0] < s + n):
+            raise ValueError(f"release of [{s}, {s + n}) overlaps free space (released twice?)")
         self.free.insert(i, (s, n))
         merged = []
         for a, ln in self.free:

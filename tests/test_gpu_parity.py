@@ -96,6 +96,22 @@ def test_dense_lists_many_pair_windows(n_beads, lanes):
     assert hdr[:, 1].max() > 64
 
 
+@pytest.mark.parametrize("lanes", [8, 32])
+def test_energy_only_equals_energy_with_gradient(lanes):
+    """The reference's self-consistency check (energy-only and value-and-grad
+    totals agree, test-nb-energrad-plateau.py:357,365,372): here the energy
+    of an evaluation without gradient output is the same, bit for bit."""
+    A = _engine()
+    c = small_case(seed=41, n_poses=80)
+    grid = to_device_grid(c)
+    wl = _wl(A, grid, c["lig"], c["gt"], c["lt"], len(c["poses"]), lanes)
+    poses = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
+    E1, G1, _ = A.energrad(wl, poses, grad=True)
+    E0, G0, _ = A.energrad(wl, poses, grad=False)
+    assert G0 is None and G1 is not None
+    assert torch.equal(E0, E1)
+
+
 @pytest.mark.parametrize("what", ["grid_only", "nb_only", "inner_only"])
 def test_energrad_partial_grids(what):
     A = _engine()

@@ -1,6 +1,8 @@
 """The oracle against the reference's golden vectors (CPU only)."""
 import numpy as np
 import pytest
+from hypothesis import given, settings
+from hypothesis import strategies as st
 
 import attract_oracle as O
 from conftest import dat_poses, mono_leu_setup
@@ -158,3 +160,26 @@ def test_euler_gradient_consistent_with_mat_gradient(golden, nb_plat):
         dmat = (O.pose_to_mat(pp) - O.pose_to_mat(pm)) / (2 * h)
         chain = (dmat[:, :3, :3] * dM[:, :3, :3]).sum((1, 2))
         assert np.allclose(chain, g[:, k], rtol=1e-6, atol=1e-4)
+
+
+@settings(max_examples=25, deadline=None)
+@given(seed=st.integers(0, 10_000), shift=st.tuples(*[st.floats(-20.0, 20.0)] * 3))
+def test_oracle_energy_is_translation_invariant(seed, shift):
+    """Moving the receptor, the grid origin and every pose by the same vector
+    leaves the oracle's energies and pose gradients unchanged (FP64): the
+    grid, list and pair terms depend only on relative positions."""
+    from gpu_cases import small_case
+
+    c = small_case(seed=seed, n_poses=12)
+    G = c["G"]
+    v = np.asarray(shift)
+    G2 = dict(G)
+    G2["geom"] = dict(G["geom"], origin=np.asarray(G["geom"]["origin"]) + v)
+    G2["rec"] = G["rec"] + v
+    poses2 = c["poses"].copy()
+    poses2[:, 3:] += v
+    E1, g1 = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], G)
+    E2, g2 = O.energrad(poses2, c["lig"], c["gt"], c["lt"], G2)
+    scale = np.abs(E1) + 1.0
+    assert np.all(np.abs(E1 - E2) <= 1e-9 * scale)
+    assert np.allclose(g1, g2, rtol=1e-7, atol=1e-7 * scale.max())

@@ -2,8 +2,9 @@
 available here): every grid, list and receptor index of the scoring kernels
 is checked before its access.  On cases that reach every index path -- inner
 and outer grids, neighbour lists that overflow their 32-byte records into the
-CSR tail, a chunked large ligand, the adjoint's grid scatter, the 4x4 and
-quaternion modes -- no check fails, and the results equal the regular build's."""
+CSR tail, dense lists that fill the pair buffers many times over, a chunked
+large ligand, the adjoint's grid scatter, the 4x4 and quaternion modes -- no
+check fails, and the results equal the regular build's."""
 import json
 import os
 import subprocess
@@ -45,6 +46,15 @@ wl1 = A.Workload([grid], A.LigandSet([(c["lig"], c["gt"], c["lt"])]), [A.Segment
 Ex, Gx, _ = A.energrad(wl1, mats)
 qt = torch.zeros((64, 8), device="cuda"); qt[:, 3] = 1.0; qt[:, 4:7] = P[:64, 3:6]
 oq, Eq, _ = A.minimise_schema(wl1, qt, ((3, 0.1, True), (2, 0.05, False)))
+# dense lists (~100 entries, mostly in the CSR tail): every team's pair buffer
+# fills many times over, at 2 and 8 beads per lane
+cd = small_case(seed=31, n_rec=400, n_lig_beads=60, n_poses=16)
+gd = to_device_grid(cd)
+Ed = []
+for lanes in (32, 8):
+    wd = A.Workload([gd], A.LigandSet([(cd["lig"], cd["gt"], cd["lt"])]), [A.Segment(0, 0, 16)], lanes_per_pose=lanes)
+    Pd = torch.tensor(cd["poses"], dtype=torch.float32, device="cuda")
+    Ed += A.energrad(wd, Pd)[0].cpu().tolist() + A.minimise(wd, Pd, 3)[1].cpu().tolist()
 torch.cuda.synchronize()
 import ctypes as C
 info = (C.c_ulonglong * 3)()
@@ -52,7 +62,7 @@ _lib.check(_lib.load().att_kernel_debug_info(info, 1, torch.cuda.current_stream(
 res = dict(word=_lib.kernel_status(clear=True), debug=[int(v) for v in info], n_overflow=int((grid.nb_hdr[:, 1] > 13).sum()),
            entries=int(st[2]), E=E.cpu().tolist(), G=G.cpu().reshape(-1).tolist(), Em=Em.cpu().tolist(),
            dP=dP.cpu().reshape(-1).tolist(), di=float(di.abs().sum()), do=float(do.abs().sum()),
-           Ex=Ex.cpu().tolist(), Eq=Eq.cpu().tolist())
+           Ex=Ex.cpu().tolist(), Eq=Eq.cpu().tolist(), Ed=Ed)
 print("RESULT " + json.dumps(res))
 '''
 
@@ -76,7 +86,7 @@ def test_bounds_checked_build_finds_no_bad_index_and_matches():
     ref = _run(None)
     assert got["word"] == 0 and got["debug"] == [0, 0, 0], (got["word"], got["debug"])
     assert got["n_overflow"] > 0  # the overflow path was exercised
-    for k in ("E", "G", "Em", "dP", "Ex", "Eq"):
+    for k in ("E", "G", "Em", "dP", "Ex", "Eq", "Ed"):
         a, b = np.asarray(got[k]), np.asarray(ref[k])
         assert np.allclose(a, b, rtol=1e-5, atol=1e-4), k
     assert np.isclose(got["di"], ref["di"], rtol=1e-5) and np.isclose(got["do"], ref["do"], rtol=1e-5)

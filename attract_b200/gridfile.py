@@ -65,6 +65,8 @@ def _parse(grid_data: bytes, read_gradients: bool):
          "alphabet": np.array(h[6:105], bool), "origin": np.array(h[105:108], np.float64),
          "dim": np.array(h[108:111]), "dim2": np.array(h[111:114]), "natoms": h[114]}
     pos = _HEAD.size
+    if np.any(d["dim"] < 1) or np.any(d["dim2"] < 0):
+        raise GridFileError(f"grid dimensions {list(d['dim'])} / {list(d['dim2'])} out of range")
 
     def ints(n):
         nonlocal pos

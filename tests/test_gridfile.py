@@ -86,3 +86,40 @@ def test_grid_without_potentials_has_no_potential_fields():
     assert "inner_potential_grid" not in g._fields and "outer_potential_grid" not in g._fields
     assert g.neighbour_grid.shape == (3, 3, 3, 2)
     assert list(g.neighbour_grid.reshape(27, 2)[5]) == [2, 0]
+
+
+from hypothesis import given, settings, HealthCheck
+from hypothesis import strategies as st
+
+
+@settings(max_examples=300, deadline=None, suppress_health_check=[HealthCheck.function_scoped_fixture])
+@given(flips=st.lists(st.tuples(st.floats(0.0, 1.0, exclude_max=True), st.integers(0, 255)), max_size=6),
+       cut=st.one_of(st.none(), st.floats(0.0, 1.0)), head=st.booleans())
+def test_corrupted_grid_files_fail_cleanly(gold, flips, cut, head):
+    """Random byte changes (biased to the header, where the counts and
+    dimensions live) and truncations of a valid file: the reader returns a
+    grid or raises GridFileError, never another exception."""
+    data = bytearray(gold["grid_bytes"].tobytes())
+    span = 400 if head else len(data)
+    for where, byte in flips:
+        data[int(where * span)] = byte
+    if cut is not None:
+        data = data[:int(cut * len(data))]
+    for csr in (False, True):
+        try:
+            if csr:
+                gf.read_grid_csr(bytes(data))
+            else:
+                gf.read_grid(bytes(data), read_gradients=True)
+        except gf.GridFileError:
+            pass
+
+
+def test_negative_dimensions_are_rejected(gold):
+    """Dimensions whose signs cancel in the size check are still rejected."""
+    data = bytearray(gold["grid_bytes"].tobytes())
+    h = list(gf._HEAD.unpack_from(data, 0))
+    h[108], h[109] = -h[108], -h[109]   # dim x, y negated: same product
+    data[:gf._HEAD.size] = gf._HEAD.pack(*h)
+    with pytest.raises(gf.GridFileError, match="dimensions"):
+        gf.read_grid(bytes(data), read_gradients=True)

@@ -83,16 +83,26 @@ class ForceField:
         present, 1-based as in test5.py:128-130.  Without a selection all types
         are kept (index = ATTRACT type - 1)."""
         lines = text.splitlines()
-        potshape, ntypes = (int(x) for x in lines[0].split()[:2])
+        head = lines[0].split() if lines else []
+        if len(head) < 2:
+            raise ValueError("attract.par: the first line must hold potshape and the number of types")
+        potshape, ntypes = int(head[0]), int(head[1])
         if potshape != 8:
             raise ValueError(f"potshape {potshape} not supported (coarse-grained ATTRACT uses 8)")
+        if ntypes < 1:
+            raise ValueError(f"attract.par: {ntypes} types")
         vals = np.array(" ".join(lines[1:]).split(), dtype=np.float64)
+        if len(vals) < 3 * ntypes * ntypes:
+            raise ValueError(f"attract.par: {len(vals)} values, {3 * ntypes * ntypes} expected for {ntypes} types")
         par = vals[: 3 * ntypes * ntypes].reshape(3, ntypes, ntypes)
         rbc, abc, ipon = par
         rc = abc * rbc ** 8
         ac = abc * rbc ** 6
         sel_r = np.arange(ntypes) if rec_types is None else np.asarray(rec_types) - 1
         sel_l = np.arange(ntypes) if lig_types is None else np.asarray(lig_types) - 1
+        for name, sel in (("receptor", sel_r), ("ligand", sel_l)):
+            if sel.size and (sel.min() < 0 or sel.max() >= ntypes):
+                raise ValueError(f"attract.par: {name} types outside 1..{ntypes}")
         return cls(rc[np.ix_(sel_r, sel_l)], ac[np.ix_(sel_r, sel_l)], ipon[np.ix_(sel_r, sel_l)])
 
     @classmethod

@@ -162,3 +162,17 @@ def test_serving_launch_shapes():
     for bad in ((10, 12), (0, 32)):
         with pytest.raises(ValueError):
             launch_shape(*bad)
+
+
+def test_attract_par_errors_are_clear():
+    from attract_b200 import ForceField
+
+    good = "8 2\n" + " ".join(["1.0"] * 12)
+    ff = ForceField.from_attract_par(good)
+    assert ff.rc.shape == (2, 2)
+    for text, msg in (("", "first line"), ("7 2\n1", "potshape"), ("8 0\n", "types"),
+                      ("8 2\n" + " ".join(["1.0"] * 11), "values")):
+        with pytest.raises(ValueError, match=msg):
+            ForceField.from_attract_par(text)
+    with pytest.raises(ValueError, match="outside"):
+        ForceField.from_attract_par(good, rec_types=[1, 3])

@@ -211,11 +211,19 @@ __device__ __forceinline__ void pair_term_masked(const KParams& p, const KGrid& 
   gz = gf * dz;
 }
 
+// Blocks of 128 threads per SM: one bead per lane with 32-lane teams runs 6
+// (80 registers, one pair in flight per lane), with 8/16-lane teams 5 (their
+// minimiser would spill at 80); two beads per lane 4, more 2.  Measured on the
+// 18-30-bead config-1 mix: 6 blocks with one pair in flight beat 5 blocks with
+// two by 6 %; with two beads per lane, one pair in flight lost 7-14 %.
+template <int S, int K>
+__host__ __device__ constexpr int score_blocks_per_sm() { return K == 1 ? (S == 32 ? 6 : 5) : K == 2 ? 4 : 2; }
+
 template <int S, int K, int MODE>
-__global__ void __launch_bounds__(128, (K == 1 ? 5 : K == 2 ? 4 : 2)) score_kernel(const __grid_constant__ KParams p) {
+__global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kernel(const __grid_constant__ KParams p) {
   constexpr int P = 32 / S;      // poses per warp
   constexpr int NB = S * K;      // bead slots per pose
-  constexpr int U = 2;           // pair slots in flight per lane
+  constexpr int U = K == 1 ? 1 : 2;  // pair slots in flight per lane
   constexpr int PB = pairs_per_bead(K) * NB;  // pair-buffer window of one team
   constexpr bool MAT = (MODE == MODE_EVAL_MAT);
   constexpr bool QUAT = (MODE == MODE_QUAT);   // quaternion + adabelief SCHEMA protocol

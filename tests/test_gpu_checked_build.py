@@ -2,8 +2,8 @@
 available here): every grid, list and receptor index of the scoring kernels
 is checked before its access.  On cases that reach every index path -- inner
 and outer grids, neighbour lists that overflow their 32-byte records into the
-CSR tail, dense lists that fill the pair buffers many times over, a chunked
-large ligand, the adjoint's grid scatter, the 4x4 and quaternion modes -- no
+CSR tail, dense lists that fill the pair buffers many times over, two
+receptors and ligands of 5 to 60 beads in one launch, a chunked large ligand, the adjoint's grid scatter, the 4x4 and quaternion modes -- no
 check fails, and the results equal the regular build's."""
 import json
 import os
@@ -55,6 +55,18 @@ for lanes in (32, 8):
     wd = A.Workload([gd], A.LigandSet([(cd["lig"], cd["gt"], cd["lt"])]), [A.Segment(0, 0, 16)], lanes_per_pose=lanes)
     Pd = torch.tensor(cd["poses"], dtype=torch.float32, device="cuda")
     Ed += A.energrad(wd, Pd)[0].cpu().tolist() + A.minimise(wd, Pd, 3)[1].cpu().tolist()
+# two receptors in one launch (segments on either grid) and ligands of 5 to 60 beads,
+# as the serving rounds launch them
+c2 = small_case(seed=96, n_rec=120, n_poses=16)
+g2 = to_device_grid(c2)
+rngm = np.random.default_rng(8)
+mix = [(rngm.normal(size=(n, 3)) * 2.0, rngm.integers(0, 4, n)) for n in (5, 17, 33, 60)]
+Emix = []
+for lanes in (8, 32):
+    wm = A.Workload([grid, g2], A.LigandSet([(x, t, t) for x, t in mix]),
+                    [A.Segment(i % 2, i, 16) for i in range(len(mix))], lanes_per_pose=lanes)
+    Pm = torch.tensor(np.concatenate([c["poses"][:16]] * len(mix)), dtype=torch.float32, device="cuda")
+    Emix += A.energrad(wm, Pm)[0].cpu().tolist() + A.minimise(wm, Pm, 3)[1].cpu().tolist()
 torch.cuda.synchronize()
 import ctypes as C
 info = (C.c_ulonglong * 3)()
@@ -62,7 +74,7 @@ _lib.check(_lib.load().att_kernel_debug_info(info, 1, torch.cuda.current_stream(
 res = dict(word=_lib.kernel_status(clear=True), debug=[int(v) for v in info], n_overflow=int((grid.nb_hdr[:, 1] > 13).sum()),
            entries=int(st[2]), E=E.cpu().tolist(), G=G.cpu().reshape(-1).tolist(), Em=Em.cpu().tolist(),
            dP=dP.cpu().reshape(-1).tolist(), di=float(di.abs().sum()), do=float(do.abs().sum()),
-           Ex=Ex.cpu().tolist(), Eq=Eq.cpu().tolist(), Ed=Ed)
+           Ex=Ex.cpu().tolist(), Eq=Eq.cpu().tolist(), Ed=Ed, Emix=Emix)
 print("RESULT " + json.dumps(res))
 '''
 
@@ -86,7 +98,7 @@ def test_bounds_checked_build_finds_no_bad_index_and_matches():
     ref = _run(None)
     assert got["word"] == 0 and got["debug"] == [0, 0, 0], (got["word"], got["debug"])
     assert got["n_overflow"] > 0  # the overflow path was exercised
-    for k in ("E", "G", "Em", "dP", "Ex", "Eq", "Ed"):
+    for k in ("E", "G", "Em", "dP", "Ex", "Eq", "Ed", "Emix"):
         a, b = np.asarray(got[k]), np.asarray(ref[k])
         assert np.allclose(a, b, rtol=1e-5, atol=1e-4), k
     assert np.isclose(got["di"], ref["di"], rtol=1e-5) and np.isclose(got["do"], ref["do"], rtol=1e-5)

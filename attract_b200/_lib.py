@@ -21,6 +21,7 @@ ATT_STATUS_NONFINITE_POSE = 4
 ATT_MAX_GRIDS = 8
 ATT_KERR_COPY_TIMEOUT = 1
 ATT_KERR_BOUNDS = 2
+ATT_KERR_BAD_SEGMENT = 4
 ATT_TEST_STALL_COPY_WAIT = 1
 ATT_NB_EMPTY = 65535
 
@@ -44,7 +45,8 @@ class AttGrid(C.Structure):
 
 
 class AttLigands(C.Structure):
-    _fields_ = [("beads", C.c_void_p), ("offset", C.c_void_p), ("n_lig", C.c_int), ("max_beads", C.c_int)]
+    _fields_ = [("beads", C.c_void_p), ("offset", C.c_void_p), ("n_lig", C.c_int), ("max_beads", C.c_int),
+                ("n_beads", C.c_int), ("pad_", C.c_int)]
 
 
 class AttSegment(C.Structure):
@@ -85,11 +87,11 @@ SIGNATURES = {
     "att_version": (C.c_char_p, []),
     "att_grid_brick_bytes": (LL, [C.POINTER(AttGridGeom), I]),
     "att_grid_repack": (I, [C.POINTER(AttGridGeom), P, P, P, P]),
-    "att_energrad": (I, [C.POINTER(AttGrid), I, C.POINTER(AttLigands), P, I, P, I, P, P,
+    "att_energrad": (I, [C.POINTER(AttGrid), I, C.POINTER(AttLigands), P, I, P, I, I, P, P,
                          C.POINTER(AttEvalCfg), P, P, P, C.POINTER(AttLaunchCfg), P]),
-    "att_minimise": (I, [C.POINTER(AttGrid), I, C.POINTER(AttLigands), P, I, P, I, P, P, P, P,
+    "att_minimise": (I, [C.POINTER(AttGrid), I, C.POINTER(AttLigands), P, I, P, I, I, P, P, P, P,
                          C.POINTER(AttAdamCfg), I, P, P, P, P, C.POINTER(AttLaunchCfg), P]),
-    "att_energrad_backward": (I, [C.POINTER(AttGrid), I, C.POINTER(AttLigands), P, I, P, I, P, P,
+    "att_energrad_backward": (I, [C.POINTER(AttGrid), I, C.POINTER(AttLigands), P, I, P, I, I, P, P,
                                   C.POINTER(AttEvalCfg), P, P, P, P, C.POINTER(AttLaunchCfg), P]),
     "att_build_potential_grid": (I, [C.POINTER(AttGridGeom), P, I, P, I, I, F, I, P, P]),
     "att_nbgrid_workspace_bytes": (LL, [LL]),
@@ -100,7 +102,7 @@ SIGNATURES = {
     "att_nbgrid_pack_records": (I, [P, P, LL, I, P, P]),
     "att_kernel_debug_info": (I, [C.POINTER(C.c_ulonglong), I, P]),
     "att_allpairs_energy": (I, [P, I, P, I, P, I, I, P, I, I, F, P, P, P]),
-    "att_minimise_schema": (I, [C.POINTER(AttGrid), I, C.POINTER(AttLigands), P, I, P, I, P, P, P,
+    "att_minimise_schema": (I, [C.POINTER(AttGrid), I, C.POINTER(AttLigands), P, I, P, I, I, P, P, P,
                                 C.POINTER(AttSchemaCfg), P, P, P, C.POINTER(AttLaunchCfg), P]),
 }
 

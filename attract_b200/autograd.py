@@ -37,6 +37,7 @@ class DockingEnergy(torch.autograd.Function):
         E, _, _ = energrad(wl, poses.detach().contiguous(), opts, grad=False)
         ctx.save_for_backward(poses)
         ctx.wl, ctx.opts = wl, opts
+        ctx.packed_version = getattr(grid, "_packed_version", None)
         ctx.has_inner, ctx.has_outer = inner is not None, outer is not None
         return E
 
@@ -45,6 +46,11 @@ class DockingEnergy(torch.autograd.Function):
         (poses,) = ctx.saved_tensors
         wl, opts = ctx.wl, ctx.opts
         grid = wl.grids[0]
+        if getattr(grid, "_packed_version", None) != ctx.packed_version:
+            # the backward recomputes the forward from the bricks: another
+            # forward repacked them from modified dense grids in between
+            raise RuntimeError("the grid's bricks were repacked from modified dense grids after this forward; "
+                               "its backward would use the new grid values")
         need_grid = ctx.needs_input_grad[1] or ctx.needs_input_grad[2]
         din = torch.zeros_like(grid.inner) if (need_grid and ctx.has_inner) else None
         dout = torch.zeros_like(grid.outer) if (need_grid and ctx.has_outer) else None

@@ -3,8 +3,11 @@
 Candidates are (lanes per pose, threads per block): 8/16/32 lanes per pose
 (4/2/1 poses per warp) x 64/128 threads.  Each candidate minimises a sample
 of every segment for a few steps, timed with CUDA events; the fastest wins and
-is cached per (GPU, bead-count histogram) in a JSON file
-(``$ATTRACT_B200_CACHE`` or ``~/.cache/attract_b200/autotune.json``).
+is cached in a JSON file (``$ATTRACT_B200_CACHE`` or
+``~/.cache/attract_b200/autotune.json``) under a key of what decides the
+winner: the GPU, the ligand bead counts, and a binned histogram of the
+grids' neighbour-list lengths (long lists shift the balance between the
+per-bead and the per-pair work).
 """
 from __future__ import annotations
 
@@ -18,6 +21,8 @@ from ._lib import AttractError
 from .engine import AdamOptions, EvalOptions, LaunchShape, Segment, Workload, minimise
 
 CANDIDATES = [(8, 64), (8, 128), (16, 64), (16, 128), (32, 64), (32, 128)]
+# list-length bins of the cache key: empty, 1-5, 6-10, 11-20, 21-40, more
+LIST_BINS = (0, 1, 6, 11, 21, 41)
 
 
 def _cache_path() -> str:
@@ -25,10 +30,75 @@ def _cache_path() -> str:
                                                               "autotune.json"))
 
 
+def list_histogram(counts) -> tuple:
+    """Fractions of list-grid points per LIST_BINS bin, rounded to 0.05 so that
+    receptors of the same kind share a key."""
+    c = np.asarray(counts, np.int64).reshape(-1)
+    if c.size == 0:
+        return tuple(0.0 for _ in LIST_BINS)
+    idx = np.searchsorted(np.asarray(LIST_BINS), c, side="right") - 1
+    frac = np.bincount(idx, minlength=len(LIST_BINS)) / c.size
+    return tuple(float(round(f * 20) / 20) for f in frac)
+
+
+def grid_list_histogram(grid) -> tuple:
+    """:func:`list_histogram` of a Grid's neighbour lists (cached on the grid)."""
+    h = getattr(grid, "_list_hist", None)
+    if h is None:
+        if grid.nb_hdr is None:
+            h = list_histogram([])
+        else:
+            cnt = grid.nb_hdr[:, 1].to(torch.int64)
+            edges = torch.tensor(LIST_BINS[1:], dtype=torch.int64, device=cnt.device)
+            idx = torch.bucketize(cnt, edges, right=True)
+            frac = torch.bincount(idx, minlength=len(LIST_BINS)).cpu().numpy() / max(cnt.numel(), 1)
+            h = tuple(float(round(f * 20) / 20) for f in frac)
+        grid._list_hist = h
+    return h
+
+
+def cache_key(device_name: str, bead_sizes, list_hists) -> str:
+    """The autotuner's cache key: GPU, sorted distinct bead counts, and the
+    list-length histogram of every grid the workload uses."""
+    sizes = ",".join(str(int(n)) for n in sorted(set(int(x) for x in bead_sizes)))
+    hists = ";".join(",".join(f"{f:.2f}" for f in h) for h in list_hists)
+    return f"{device_name}|beads={sizes}|lists={hists}"
+
+
 def _key(wl: Workload) -> str:
     name = torch.cuda.get_device_name(wl.device)
-    sizes = sorted(set(int(wl.ligands.sizes[s.lig]) for s in wl.segments if s.n_poses))
-    return f"{name}|{','.join(map(str, sizes))}"
+    sizes = [wl.ligands.sizes[s.lig] for s in wl.segments if s.n_poses]
+    used = sorted(set(s.grid for s in wl.segments if s.n_poses))
+    return cache_key(name, sizes, [grid_list_histogram(wl.grids[g]) for g in used])
+
+
+def cache_lookup(path: str, key: str):
+    """(LaunchShape, timings) cached under ``key`` in ``path``, or None."""
+    if not os.path.exists(path):
+        return None
+    try:
+        hit = json.load(open(path)).get(key)
+    except (OSError, ValueError):
+        return None
+    if not hit:
+        return None
+    return LaunchShape(int(hit["lanes"]), int(hit["threads"])), hit.get("ms", {})
+
+
+def cache_store(path: str, key: str, shape: LaunchShape, times: dict) -> None:
+    """Add or replace ``key`` in the JSON cache file (other keys are kept)."""
+    try:
+        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+        try:
+            data = json.load(open(path)) if os.path.exists(path) else {}
+        except ValueError:
+            data = {}
+        data[key] = dict(lanes=shape.lanes_per_pose, threads=shape.block_threads, ms=times)
+        tmp = path + ".tmp"
+        json.dump(data, open(tmp, "w"), indent=1)
+        os.replace(tmp, path)
+    except OSError:
+        pass
 
 
 def autotune(wl: Workload, poses: torch.Tensor, steps: int = 10, sample: int = 65536,
@@ -37,13 +107,10 @@ def autotune(wl: Workload, poses: torch.Tensor, steps: int = 10, sample: int = 6
     """Pick the fastest launch shape for ``wl``; returns (shape, timings in ms)."""
     key = _key(wl)
     path = _cache_path()
-    if use_cache and os.path.exists(path):
-        try:
-            hit = json.load(open(path)).get(key)
-            if hit:
-                return LaunchShape(hit["lanes"], hit["threads"]), hit.get("ms", {})
-        except (OSError, ValueError):
-            pass
+    if use_cache:
+        hit = cache_lookup(path, key)
+        if hit is not None:
+            return hit
     # a sample of each segment, same bead-count mix
     segs, parts = [], []
     for s, p0 in zip(wl.segments, wl.pose0):
@@ -73,12 +140,7 @@ def autotune(wl: Workload, poses: torch.Tensor, steps: int = 10, sample: int = 6
     if not times:
         raise AttractError("no candidate launch shape fits this workload's shared memory")
     lanes, threads = (int(x) for x in min(times, key=times.get).split("x"))
+    shape = LaunchShape(lanes, threads)
     if use_cache:
-        try:
-            os.makedirs(os.path.dirname(path), exist_ok=True)
-            data = json.load(open(path)) if os.path.exists(path) else {}
-            data[key] = dict(lanes=lanes, threads=threads, ms=times)
-            json.dump(data, open(path, "w"), indent=1)
-        except (OSError, ValueError):
-            pass
-    return LaunchShape(lanes, threads), times
+        cache_store(path, key, shape, times)
+    return shape, times

@@ -95,14 +95,22 @@ cudaError_t launch_build_potential(const AttGridGeom& g, const float* rec, int n
 // ---------------------------------------------------------------------------
 constexpr int SCAN_THREADS = 1024;
 
+// Grid point and squared distance with every operation rounded on its own
+// (no contraction into FMA): the list membership test d^2 <= r^2 is then a
+// fixed float32 computation that a host restatement reproduces bit for bit.
 __device__ __forceinline__ void point_of(const AttGridGeom& g, long long v, float& x, float& y, float& z) {
   const int nz = g.dim[2], ny = g.dim[1];
   const int iz = (int)(v % nz);
   const int iy = (int)((v / nz) % ny);
   const int ix = (int)(v / ((long long)nz * ny));
-  x = g.origin[0] + ix * g.spacing;
-  y = g.origin[1] + iy * g.spacing;
-  z = g.origin[2] + iz * g.spacing;
+  x = __fadd_rn(g.origin[0], __fmul_rn((float)ix, g.spacing));
+  y = __fadd_rn(g.origin[1], __fmul_rn((float)iy, g.spacing));
+  z = __fadd_rn(g.origin[2], __fmul_rn((float)iz, g.spacing));
+}
+
+__device__ __forceinline__ float dist2_rn(float x, float y, float z, const float4& r) {
+  const float dx = __fsub_rn(x, r.x), dy = __fsub_rn(y, r.y), dz = __fsub_rn(z, r.z);
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
 }
 
 // count + block-local exclusive scan; block totals to ws
@@ -121,9 +129,7 @@ nb_count_kernel(AttGridGeom g, const float4* __restrict__ rec, int n_rec, float 
     __syncthreads();
     const int m = min(SCAN_THREADS, n_rec - base);
     for (int k = 0; k < m; ++k) {
-      const float4 r = srec[k];
-      const float dx = x - r.x, dy = y - r.y, dz = z - r.z;
-      c += (dx * dx + dy * dy + dz * dz) <= r2;
+      c += dist2_rn(x, y, z, srec[k]) <= r2;
     }
   }
   if (v >= nvox) c = 0;
@@ -214,9 +220,7 @@ nb_fill_kernel(AttGridGeom g, const float4* __restrict__ rec, int n_rec, float r
     const int m = min(256, n_rec - base);
     if (v >= nvox) continue;
     for (int k = 0; k < m; ++k) {
-      const float4 r = srec[k];
-      const float dx = x - r.x, dy = y - r.y, dz = z - r.z;
-      if ((dx * dx + dy * dy + dz * dz) <= r2 && pos < h.y) list[h.x + pos++] = (uint16_t)(base + k);
+      if (dist2_rn(x, y, z, srec[k]) <= r2 && pos < h.y) list[h.x + pos++] = (uint16_t)(base + k);
     }
   }
 }
@@ -317,6 +321,7 @@ cudaError_t launch_repack(const AttGridGeom& g, const float* inner, const float*
 
 namespace att {
 int report_error(int code, const char* msg);
+int check_geom(const AttGridGeom* g);  // the validation of att_nbgrid_count (capi.cu)
 }
 
 // Fixed scan workspace: 8192 words = 32 KB, i.e. grids of up to 8192 * 1024
@@ -326,20 +331,47 @@ static __device__ __align__(256) unsigned g_nbgrid_scan_ws[ATT_NBGRID_NOALLOC_MA
 namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_scan_ws_mutex;
-void* g_scan_ws_addr[kMaxDevices] = {};  // device address of g_nbgrid_scan_ws, per device
+struct ScanWsEntry {
+  void* ctx;   // the CUDA context the address belongs to
+  void* addr;  // device address of g_nbgrid_scan_ws in that context
+};
+ScanWsEntry g_scan_ws[kMaxDevices] = {};
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link-time
+// dependency on the driver library); NULL when unavailable.
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  return fn;
+}
 
 // Device address of the fixed workspace on the current device.  The name
 // g_nbgrid_scan_ws in host code is only a host-side stand-in for the symbol;
-// the kernel must be given the address that cudaGetSymbolAddress returns for
-// the device that is current.  Looked up once per device, on the first call.
+// the kernel must be given the address that cudaGetSymbolAddress returns with
+// that device current.  Looked up on the first call on a device and cached per
+// device together with the context it was taken in: after a device reset (or
+// with another context current) the stale address is dropped and looked up
+// again.  Without a current context handle (none made current yet, or no
+// driver entry point) the address is looked up on every call.
 int scan_ws_address(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return att::report_error(ATT_E_CUDA, "att_nbgrid_count_noalloc: cudaGetDevice failed");
   if (dev < 0 || dev >= kMaxDevices)
     return att::report_error(ATT_E_UNSUPPORTED, "att_nbgrid_count_noalloc: device index beyond 64");
+  void* ctx = nullptr;
+  CtxGetCurrentFn get = ctx_get_current();
+  const bool have_ctx = get != nullptr && get(&ctx) == 0 && ctx != nullptr;
   std::lock_guard<std::mutex> lock(g_scan_ws_mutex);
-  if (g_scan_ws_addr[dev] == nullptr) {
+  ScanWsEntry& ent = g_scan_ws[dev];
+  if (!have_ctx || ent.addr == nullptr || ent.ctx != ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_nbgrid_scan_ws);
     if (e != cudaSuccess || p == nullptr) {
@@ -348,9 +380,10 @@ int scan_ws_address(void** out) {
                cudaGetErrorString(e));
       return att::report_error(ATT_E_CUDA, msg);
     }
-    g_scan_ws_addr[dev] = p;
+    ent.addr = p;
+    ent.ctx = have_ctx ? ctx : nullptr;
   }
-  *out = g_scan_ws_addr[dev];
+  *out = ent.addr;
   return ATT_OK;
 }
 }  // namespace
@@ -358,11 +391,8 @@ int scan_ws_address(void** out) {
 extern "C" int att_nbgrid_count_noalloc(const AttGridGeom* geom, const float* rec_dev, int n_rec, float radius,
                                         uint32_t* hdr_dev, unsigned long long* total_dev, void* stream) {
   char msg[256];
-  if (geom == nullptr) return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: geometry is NULL");
-  for (int k = 0; k < 3; ++k) {
-    if (geom->dim[k] < 2) return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: dim must be >= 2");
-  }
-  if (!(geom->spacing > 0.f)) return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: spacing must be > 0");
+  int rc = att::check_geom(geom);  // the same geometry rules as att_nbgrid_count
+  if (rc != ATT_OK) return rc;
   const long long nvox = (long long)geom->dim[0] * geom->dim[1] * geom->dim[2];
   if (nvox > ATT_NBGRID_NOALLOC_MAX_VOXELS) {
     snprintf(msg, sizeof(msg),
@@ -377,7 +407,7 @@ extern "C" int att_nbgrid_count_noalloc(const AttGridGeom* geom, const float* re
     return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: NULL output");
   if (!(radius >= 0.f)) return att::report_error(ATT_E_INVALID, "att_nbgrid_count_noalloc: radius < 0");
   void* ws = nullptr;
-  int rc = scan_ws_address(&ws);
+  rc = scan_ws_address(&ws);
   if (rc != ATT_OK) return rc;
   // every workspace word the scan reads is written by the count kernel of the
   // same call first, so nothing has to be cleared between calls

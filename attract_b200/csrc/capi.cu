@@ -61,7 +61,9 @@ static bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_
 // static grid-descriptor copies (ATT_MAX_GRIDS KGrid) and slack
 static const size_t kDynSmemLimit = 227 * 1024 - 4096;
 
-static int check_geom(const AttGridGeom* g) {
+namespace att {
+// geometry validation shared by every entry point that takes an AttGridGeom
+int check_geom(const AttGridGeom* g) {
   REQUIRE(g != nullptr, "geometry is NULL");
   for (int k = 0; k < 3; ++k) {
     REQUIRE(g->dim[k] >= 2, "dim[%d] = %d must be >= 2", k, g->dim[k]);
@@ -72,6 +74,7 @@ static int check_geom(const AttGridGeom* g) {
   REQUIRE(g->n_types >= 1 && g->n_types <= 65535, "n_types = %d out of range", g->n_types);
   return ATT_OK;
 }
+}  // namespace att
 
 long long att_grid_brick_bytes(const AttGridGeom* g, int with_outer) {
   if (check_geom(g) != ATT_OK) return -1;
@@ -164,7 +167,8 @@ static int make_kgrid(const AttGrid* a, int gi, KGrid* k) {
 }
 
 static int fill_common(KParams* p, const AttGrid* grids, int n_grids, const AttLigands* ligs,
-                       const AttSegment* segs, int n_segs, const int* seg_tile, int n_tiles, const float* pose,
+                       const AttSegment* segs, int n_segs, const int* seg_tile, int n_tiles, int n_pose_rows,
+                       const float* pose,
                        const int* pose_lig, const AttEvalCfg* cfg, const AttLaunchCfg* launch, int* S, int* K,
                        int* threads) {
   REQUIRE(grids != nullptr && n_grids >= 1 && n_grids <= ATT_MAX_GRIDS, "n_grids = %d out of range [1, %d]",
@@ -174,6 +178,7 @@ static int fill_common(KParams* p, const AttGrid* grids, int n_grids, const AttL
   REQUIRE(aligned(ligs->beads, 16), "ligand beads not 16-B aligned");
   REQUIRE(segs != nullptr && n_segs >= 1 && seg_tile != nullptr, "segments / seg_tile missing");
   REQUIRE(n_tiles >= 0, "n_tiles < 0");
+  REQUIRE(n_pose_rows >= 0, "n_pose_rows < 0");
   REQUIRE(pose != nullptr || n_tiles == 0, "pose is NULL");
   REQUIRE(cfg != nullptr, "eval cfg is NULL");
   REQUIRE(cfg->grad_mode == ATT_GRAD_REFERENCE || cfg->grad_mode == ATT_GRAD_ANALYTIC, "grad_mode %d unknown",
@@ -182,6 +187,8 @@ static int fill_common(KParams* p, const AttGrid* grids, int n_grids, const AttL
   REQUIRE(s == 8 || s == 16 || s == 32, "lanes_per_pose = %d (8, 16 or 32)", s);
   *S = s;
   REQUIRE(ligs->max_beads >= 1, "ligands: max_beads = %d", ligs->max_beads);
+  REQUIRE(ligs->n_beads >= ligs->max_beads, "ligands: n_beads = %d < max_beads = %d", ligs->n_beads,
+          ligs->max_beads);
   *K = beads_per_lane(s, ligs->max_beads);
   int t = (launch && launch->block_threads) ? launch->block_threads : 128;
   REQUIRE(t == 32 || t == 64 || t == 96 || t == 128, "block_threads = %d (32, 64, 96 or 128)", t);
@@ -207,6 +214,11 @@ static int fill_common(KParams* p, const AttGrid* grids, int n_grids, const AttL
   p->seg_tile = seg_tile;
   p->n_segs = n_segs;
   p->n_tiles = n_tiles;
+  p->n_grids = n_grids;
+  p->n_lig = ligs->n_lig;
+  p->max_beads = ligs->max_beads;
+  p->n_lig_beads = ligs->n_beads;
+  p->n_pose_rows = n_pose_rows;
   p->pose_in = pose;
   p->pose_lig = pose_lig;
   p->grad_mode = cfg->grad_mode;
@@ -216,12 +228,12 @@ static int fill_common(KParams* p, const AttGrid* grids, int n_grids, const AttL
 }
 
 extern "C" int att_energrad(const AttGrid* grids, int n_grids, const AttLigands* ligs, const AttSegment* segs_dev,
-                            int n_segs, const int* seg_tile_dev, int n_tiles, const float* pose_dev,
+                            int n_segs, const int* seg_tile_dev, int n_tiles, int n_pose_rows, const float* pose_dev,
                             const int* pose_lig_dev, const AttEvalCfg* cfg, float* energy_dev, float* grad_dev,
                             int* status_dev, const AttLaunchCfg* launch, void* stream) {
   KParams p;
   int S = 8, K = 1, threads = 128;
-  int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, pose_dev, pose_lig_dev,
+  int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, n_pose_rows, pose_dev, pose_lig_dev,
                        cfg, launch, &S, &K, &threads);
   if (rc) return rc;
   REQUIRE(energy_dev != nullptr || n_tiles == 0, "energy output is NULL");
@@ -260,7 +272,7 @@ static int persistent_blocks(int mode, int S, int K, int threads, int rec_slot, 
 }
 
 extern "C" int att_minimise(const AttGrid* grids, int n_grids, const AttLigands* ligs, const AttSegment* segs_dev,
-                            int n_segs, const int* seg_tile_dev, int n_tiles, const float* pose_in_dev,
+                            int n_segs, const int* seg_tile_dev, int n_tiles, int n_pose_rows, const float* pose_in_dev,
                             float* pose_out_dev, const int* pose_lig_dev, float* adam_state_dev,
                             const AttAdamCfg* cfg, int steps, float* energy_dev, int* status_dev,
                             int* work_counter_dev, unsigned long long* stats_dev, const AttLaunchCfg* launch,
@@ -268,7 +280,7 @@ extern "C" int att_minimise(const AttGrid* grids, int n_grids, const AttLigands*
   REQUIRE(cfg != nullptr, "adam cfg is NULL");
   KParams p;
   int S = 8, K = 1, threads = 128;
-  int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, pose_in_dev,
+  int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, n_pose_rows, pose_in_dev,
                        pose_lig_dev, &cfg->eval, launch, &S, &K, &threads);
   if (rc) return rc;
   REQUIRE(cfg->eval.pose_format == 0, "att_minimise takes Euler poses (pose_format 0)");
@@ -306,13 +318,13 @@ extern "C" int att_minimise(const AttGrid* grids, int n_grids, const AttLigands*
 
 extern "C" int att_minimise_schema(const AttGrid* grids, int n_grids, const AttLigands* ligs,
                                    const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
-                                   const float* pose_in_dev, float* pose_out_dev, const int* pose_lig_dev,
+                                   int n_pose_rows, const float* pose_in_dev, float* pose_out_dev, const int* pose_lig_dev,
                                    const AttSchemaCfg* cfg, float* energy_dev, int* status_dev,
                                    int* work_counter_dev, const AttLaunchCfg* launch, void* stream) {
   REQUIRE(cfg != nullptr, "schema cfg is NULL");
   KParams p;
   int S = 8, K = 1, threads = 128;
-  int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, pose_in_dev,
+  int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, n_pose_rows, pose_in_dev,
                        pose_lig_dev, &cfg->eval, launch, &S, &K, &threads);
   if (rc) return rc;
   REQUIRE(cfg->n_stages >= 1 && cfg->n_stages <= ATT_MAX_STAGES, "n_stages = %d (1..%d)", cfg->n_stages,
@@ -357,12 +369,12 @@ extern "C" int att_minimise_schema(const AttGrid* grids, int n_grids, const AttL
 
 extern "C" int att_energrad_backward(const AttGrid* grids, int n_grids, const AttLigands* ligs,
                                      const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
-                                     const float* pose_dev, const int* pose_lig_dev, const AttEvalCfg* cfg,
+                                     int n_pose_rows, const float* pose_dev, const int* pose_lig_dev, const AttEvalCfg* cfg,
                                      const float* dL_dE_dev, float* dL_dpose_dev, float* dgrid_inner_dev,
                                      float* dgrid_outer_dev, const AttLaunchCfg* launch, void* stream) {
   KParams p;
   int S = 8, K = 1, threads = 128;
-  int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, pose_dev, pose_lig_dev,
+  int rc = fill_common(&p, grids, n_grids, ligs, segs_dev, n_segs, seg_tile_dev, n_tiles, n_pose_rows, pose_dev, pose_lig_dev,
                        cfg, launch, &S, &K, &threads);
   if (rc) return rc;
   REQUIRE(cfg->pose_format == 0, "att_energrad_backward takes Euler poses (pose_format 0)");

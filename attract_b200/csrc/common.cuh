@@ -46,6 +46,8 @@ struct KParams {
   const AttSegment* segs;
   const int* seg_tile;
   int n_segs, n_tiles;
+  int n_grids, n_lig, max_beads;  // bounds of the segment / conformer / bead-range checks
+  int n_pose_rows;
   const float* pose_in;
   float* pose_out;
   const int* pose_lig;
@@ -72,7 +74,7 @@ struct KParams {
   float qs_lr[ATT_MAX_STAGES];
   int qs_grav[ATT_MAX_STAGES];
   float eps_root;
-  long long n_lig_beads;   // sizes for ATT_BOUNDS_CHECK builds
+  long long n_lig_beads;   // rows of lig_beads
   long long n_dgrid_inner, n_dgrid_outer;
 };
 

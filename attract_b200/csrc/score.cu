@@ -280,15 +280,37 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
 
   while (tile < p.n_tiles) {
     const int si = find_segment(p, tile);
-    const AttSegment sg = p.segs[si];
+    AttSegment sg = p.segs[si];
+    // Caller-provided tables are checked before any access they index: the
+    // segment's grid, ligand and pose range, the pose's conformer index and
+    // the ligand's bead range.  A pose that fails is skipped (no output) and
+    // flagged in the device error word.
+    const bool seg_ok = ((unsigned)sg.grid < (unsigned)p.n_grids) & ((unsigned)sg.lig < (unsigned)p.n_lig) &
+                        (sg.pose0 >= 0) & (sg.n_poses >= 0) &
+                        ((long long)sg.pose0 + sg.n_poses <= (long long)p.n_pose_rows);
     const int local = (tile - __ldg(p.seg_tile + si)) * P + slot;
-    const bool valid = local < sg.n_poses;
+    bool valid = seg_ok & (local >= 0) & (local < sg.n_poses);
+    bool bad = !seg_ok;
+    if (!seg_ok) sg.grid = sg.lig = sg.pose0 = sg.step0 = 0;
     const int b = sg.pose0 + (valid ? local : 0);
     const KGrid& G = s_grid[sg.grid];
     int lig = sg.lig;
-    if (p.pose_lig != nullptr && valid) lig += __ldg(p.pose_lig + b);
+    if (p.pose_lig != nullptr && valid) {
+      lig += __ldg(p.pose_lig + b);
+      if ((unsigned)lig >= (unsigned)p.n_lig) {
+        valid = false;
+        bad = true;
+        lig = 0;
+      }
+    }
     const int loff = __ldg(p.lig_off + lig);
-    const int Ntot = valid ? __ldg(p.lig_off + lig + 1) - loff : 0;
+    int Ntot = valid ? __ldg(p.lig_off + lig + 1) - loff : 0;
+    if (valid && ((loff < 0) | (Ntot < 0) | (Ntot > p.max_beads) | ((long long)loff + Ntot > p.n_lig_beads))) {
+      valid = false;
+      bad = true;
+      Ntot = 0;
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&g_kernel_error, ATT_KERR_BAD_SEGMENT);
     // ligands larger than the team's NB bead slots are evaluated in chunks of
     // NB beads; the chunk count is warp-uniform (the chunk loop holds warp
     // barriers and shuffles)

@@ -200,7 +200,7 @@ def energrad(wl: Workload, poses: torch.Tensor, opts: EvalOptions | None = None,
     cfg = opts.to_c(1 if mat else 0)
     lc = launch.to_c()
     rc = _lib.load().att_energrad(wl.c_grids, len(wl.grids), C.byref(wl.c_ligs), _lib.ptr(wl.segs),
-                                  len(wl.segments), _lib.ptr(wl.seg_tile), wl.n_tiles, _lib.ptr(p2),
+                                  len(wl.segments), _lib.ptr(wl.seg_tile), wl.n_tiles, wl.n_poses, _lib.ptr(p2),
                                   _lib.ptr(pose_lig), C.byref(cfg), _lib.ptr(E), _lib.ptr(G), _lib.ptr(S),
                                   C.byref(lc), _stream(stream))
     _lib.check(rc, "att_energrad")
@@ -247,7 +247,7 @@ def minimise(wl: Workload, poses: torch.Tensor, steps: int, adam: AdamOptions | 
     cfg = adam.to_c(opts)
     lc = launch.to_c()
     rc = _lib.load().att_minimise(wl.c_grids, len(wl.grids), C.byref(wl.c_ligs), _lib.ptr(wl.segs),
-                                  len(wl.segments), _lib.ptr(wl.seg_tile), wl.n_tiles, _lib.ptr(poses),
+                                  len(wl.segments), _lib.ptr(wl.seg_tile), wl.n_tiles, wl.n_poses, _lib.ptr(poses),
                                   _lib.ptr(pose_out), _lib.ptr(pose_lig), _lib.ptr(adam_state), C.byref(cfg),
                                   int(steps), _lib.ptr(scratch.energy), _lib.ptr(scratch.status),
                                   _lib.ptr(scratch.counter), _lib.ptr(st), C.byref(lc), _stream(stream))
@@ -288,7 +288,7 @@ def minimise_schema(wl: Workload, poses: torch.Tensor, schema, opts: EvalOptions
     cfg.beta1, cfg.beta2, cfg.eps, cfg.eps_root = float(betas[0]), float(betas[1]), float(eps), float(eps_root)
     lc = launch.to_c()
     rc = _lib.load().att_minimise_schema(wl.c_grids, len(wl.grids), C.byref(wl.c_ligs), _lib.ptr(wl.segs),
-                                         len(wl.segments), _lib.ptr(wl.seg_tile), wl.n_tiles, _lib.ptr(poses),
+                                         len(wl.segments), _lib.ptr(wl.seg_tile), wl.n_tiles, wl.n_poses, _lib.ptr(poses),
                                          _lib.ptr(pose_out), _lib.ptr(pose_lig), C.byref(cfg),
                                          _lib.ptr(scratch.energy), _lib.ptr(scratch.status),
                                          _lib.ptr(scratch.counter), C.byref(lc), _stream(stream))
@@ -320,7 +320,7 @@ def energrad_backward(wl: Workload, poses: torch.Tensor, dL_dE: torch.Tensor, op
     cfg = opts.to_c(0)
     lc = launch.to_c()
     rc = _lib.load().att_energrad_backward(wl.c_grids, len(wl.grids), C.byref(wl.c_ligs), _lib.ptr(wl.segs),
-                                           len(wl.segments), _lib.ptr(wl.seg_tile), wl.n_tiles, _lib.ptr(poses),
+                                           len(wl.segments), _lib.ptr(wl.seg_tile), wl.n_tiles, wl.n_poses, _lib.ptr(poses),
                                            _lib.ptr(pose_lig), C.byref(cfg), _lib.ptr(dL_dE), _lib.ptr(out),
                                            _lib.ptr(dgrid_inner), _lib.ptr(dgrid_outer), C.byref(lc),
                                            _stream(stream))

@@ -337,6 +337,7 @@ class Grid:
             _lib.check(lib.att_nbgrid_count(C.byref(ngc), _lib.ptr(rec), n_rec, float(list_radius), _lib.ptr(hdr),
                                             _lib.ptr(total), _lib.ptr(ws), wsb, st), "att_nbgrid_count")
             n_ent = int(total.item())
+            check_list_total(n_ent)
             lst = torch.empty(max(n_ent, 1), dtype=torch.int16, device=dev)
             _lib.check(lib.att_nbgrid_fill(C.byref(ngc), _lib.ptr(rec), n_rec, float(list_radius), _lib.ptr(hdr),
                                            _lib.ptr(lst), st), "att_nbgrid_fill")
@@ -374,6 +375,14 @@ class Grid:
                     vals[ok] = self.rec_perm[vals[ok]]
                     lst[s0:s0 + n] = np.sort(vals)
         return f(self.inner), f(self.outer), hdr, lst
+
+
+def check_list_total(n_entries: int) -> None:
+    """The neighbour lists' CSR starts are 32-bit (``AttGrid.nb_hdr``): a grid
+    whose entry total exceeds 2**32 - 1 would wrap them, so it is refused."""
+    if n_entries > 0xFFFFFFFF:
+        raise ValueError(f"{n_entries} neighbour-list entries: the 32-bit list starts hold at most 2**32 - 1; "
+                         "use a coarser list grid (nb_refine) or a smaller list radius")
 
 
 def _alloc_bricks(geom: GridGeom, with_outer: bool, dev) -> torch.Tensor:

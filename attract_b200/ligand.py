@@ -56,5 +56,6 @@ class LigandSet:
             a.offset = _lib.ptr(self.offset)
             a.n_lig = len(self.sizes)
             a.max_beads = max(self.sizes)
+            a.n_beads = int(sum(self.sizes))
             self._att = a
         return self._att

@@ -65,6 +65,65 @@ def receptor_beads(n: int, radius: float | None = None, min_sep: float = 3.5, n_
     return xyz, types, radius
 
 
+def receptor_beads_clustered(n: int, density: float = 0.01, n_clusters: int = 40, sigma: float = 3.0,
+                             min_sep: float = 1.5, n_types: int = 32, seed: int = 0):
+    """``n`` beads in dense patches at the same mean density as
+    :func:`receptor_beads` with ``density``: ``n_clusters`` Gaussian clusters
+    (width ``sigma``) with centres uniform in the sphere and beads pairwise
+    >= ``min_sep`` apart, so that neighbour lists within 5 A range from 0
+    (between patches) to ~80 entries (patch centres)."""
+    rng = np.random.default_rng(seed)
+    radius = (n / (density * 4.0 / 3.0 * np.pi)) ** (1.0 / 3.0)
+    centres = random_in_ball(n_clusters, max(radius - 2 * sigma, 1.0), rng)
+    cell = min_sep
+    cells: dict = {}
+    pts = []
+    sep2 = min_sep * min_sep
+    per = np.full(n_clusters, n // n_clusters)
+    per[: n - per.sum()] += 1
+    for c, m in zip(centres, per):
+        placed, tries = 0, 0
+        while placed < m:
+            tries += 1
+            if tries > 2000 * m:
+                raise RuntimeError("could not place a cluster's beads")
+            p = c + rng.normal(size=3) * sigma * (1.0 + tries / (200.0 * m))  # widen if the core is full
+            key = tuple(np.floor(p / cell).astype(int))
+            if any(((p - q) @ (p - q)) < sep2 for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)
+                   for q in cells.get((key[0] + dx, key[1] + dy, key[2] + dz), ())):
+                continue
+            cells.setdefault(key, []).append(p)
+            pts.append(p)
+            placed += 1
+    xyz = np.array(pts)
+    types = rng.integers(0, n_types, n)
+    return xyz, types, float(np.linalg.norm(xyz, axis=1).max())
+
+
+# solvent-accessible surface: bead radius 2.0 A + probe 1.4 A
+SAS_RADIUS = 3.4
+
+
+def surface_points(rec_xyz, n: int, rng, shell: float = 2.0, r_s: float = SAS_RADIUS):
+    """``n`` points uniform within ``shell`` of the receptor's solvent-accessible
+    surface: the set of points at distance ``r_s`` from their nearest bead
+    (the outer envelope and the surfaces of interior cavities alike)."""
+    from scipy.spatial import cKDTree
+
+    rec = np.asarray(rec_xyz, np.float64)
+    tree = cKDTree(rec)
+    lo, hi = rec.min(0) - r_s - shell, rec.max(0) + r_s + shell
+    out = []
+    got = 0
+    while got < n:
+        q = rng.uniform(lo, hi, (max(4 * (n - got), 4096), 3))
+        d, _ = tree.query(q)
+        q = q[np.abs(d - r_s) <= shell]
+        out.append(q)
+        got += len(q)
+    return np.concatenate(out)[:n]
+
+
 def random_walk(n: int, rng, step=3.8) -> np.ndarray:
     lo, hi = (step, step) if np.isscalar(step) else step
     d = rng.normal(size=(n - 1, 3))
@@ -105,9 +164,12 @@ def _ligand(n, rng, n_types, step):
     return xyz, t, t
 
 
-def make_config(idx: int, seed: int = 0, scale: float = 1.0, n_types: int = 32) -> Config:
+def make_config(idx: int, seed: int = 0, scale: float = 1.0, n_types: int = 32, clustered: bool = False) -> Config:
     """Config ``idx`` (0..3; the serving mix is :func:`serving_mix`).  ``scale``
-    shrinks the pose counts (not the receptor, ligands or steps) for tests."""
+    shrinks the pose counts (not the receptor, ligands or steps) for tests.
+    ``clustered`` (config 2 only): the receptor's 5000 beads in dense patches at
+    the same mean density (:func:`receptor_beads_clustered`), the regime of
+    long, ragged neighbour lists."""
     rng = np.random.default_rng(seed)
     ff = ForceField.synthetic(n_types, seed)
     sc = lambda n: max(1, int(round(n * scale)))
@@ -123,14 +185,14 @@ def make_config(idx: int, seed: int = 0, scale: float = 1.0, n_types: int = 32) 
         poses = [_poses(sc(100_000), 30.0, rng) for _ in sizes]
         steps = 200
     elif idx == 2:
-        xyz, t, R = receptor_beads(5000, density=0.01, n_types=n_types, seed=seed + 1)
+        if clustered:
+            xyz, t, R = receptor_beads_clustered(5000, density=0.01, n_types=n_types, seed=seed + 1)
+        else:
+            xyz, t, R = receptor_beads(5000, density=0.01, n_types=n_types, seed=seed + 1)
         ligs = [_ligand(40, rng, n_types, 3.8)]
         n = sc(500_000)
-        # ligand centroid within 2 A of the receptor surface (the sphere)
-        d = rng.normal(size=(n, 3))
-        d /= np.linalg.norm(d, axis=1, keepdims=True)
-        r = R + rng.uniform(-2.0, 2.0, n)
-        poses = [np.concatenate([random_rotations(n, rng), d * r[:, None]], 1)]
+        # ligand centroid within 2 A of the receptor's solvent-accessible surface
+        poses = [np.concatenate([random_rotations(n, rng), surface_points(xyz, n, rng)], 1)]
         steps = 50
     elif idx == 3:
         xyz, t, R = receptor_beads(2500, radius=40.0, n_types=n_types, seed=seed + 1)
@@ -140,7 +202,8 @@ def make_config(idx: int, seed: int = 0, scale: float = 1.0, n_types: int = 32) 
     else:
         raise ValueError(f"config {idx}")
     geom = GridGeom.around((0.0, 0.0, 0.0), R, n_types=n_types)
-    return Config(f"config{idx}", ff, xyz, t, R, geom, ligs, poses, steps)
+    return Config(f"config{idx}" + ("-clustered" if clustered and idx == 2 else ""), ff, xyz, t, R, geom, ligs, poses,
+                  steps)
 
 
 def serving_mix(seed: int = 0, n_types: int = 32, sizes=(1500, 3000, 4500, 6000)):

@@ -54,6 +54,14 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="length of the serving run (0 = skip; the full serving workload is 600 s)")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="request arrivals per second")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run only the minimiser on one configuration, --launches times (for ncu captures)")
+    ap.add_argument("--config", type=int, default=1, help="--profile-case: configuration (0, 1 or 2)")
+    ap.add_argument("--clustered", action="store_true", help="--profile-case: config 2's clustered receptor")
+    ap.add_argument("--types", type=int, default=32, help="--profile-case: ligand types (grid size)")
+    ap.add_argument("--launches", type=int, default=3, help="--profile-case: minimiser launches")
+    ap.add_argument("--refine", type=int, default=4, help="--profile-case: neighbour-list grid refinement")
+    ap.add_argument("--adam-steps", type=int, default=-1, help="--profile-case: ADAM steps (-1: the config's)")
     return ap.parse_args()
 
 
@@ -232,10 +240,15 @@ def other_configs(args, device, shape):
     from attract_b200.poses import euler_to_Q
 
     res = {}
-    names = {0: "plain small: 1200-bead receptor, 7-bead fragment, 4096 poses, 1 eval + 100 ADAM steps",
-             2: "nbgrid-heavy: 5000 beads at 0.01/A^3, 40-bead ligand, 500000 surface poses, 1 eval + 50 ADAM"}
-    for idx in (0, 2):
-        cfg = synth.make_config(idx, seed=0, scale=args.scale)
+    names = {"config0": "plain small: 1200-bead receptor, 7-bead fragment, 4096 poses, 1 eval + 100 ADAM steps",
+             "config2": "nbgrid-heavy: 5000 beads at 0.01/A^3 (uniform, 3.5 A apart), 40-bead ligand, 500000 poses "
+                        "with the centroid within 2 A of the solvent-accessible surface (probe 1.4 A + bead 2.0 A, "
+                        "outer envelope and cavities), 1 eval + 50 ADAM",
+             "config2_clustered": "nbgrid-heavy, clustered: the same 5000 beads in 40 dense patches (Gaussian, "
+                                  "3 A wide, 1.5 A apart) at the same mean density, so lists of 0-80 entries; "
+                                  "40-bead ligand, 500000 surface poses, 1 eval + 50 ADAM"}
+    for key, idx, clustered in (("config0", 0, False), ("config2", 2, False), ("config2_clustered", 2, True)):
+        cfg = synth.make_config(idx, seed=0, scale=args.scale, clustered=clustered)
         grid = A.Grid.build(cfg.rec_xyz, cfg.rec_type, cfg.ff, cfg.geom, cutoff=cfg.cutoff, device=device)
         ligs = A.LigandSet(cfg.ligands, device=device)
         poses_np = np.concatenate(cfg.poses).astype(np.float32)
@@ -248,10 +261,12 @@ def other_configs(args, device, shape):
         scratch = A.MinimiseScratch(wl.n_poses, device)
         out = torch.empty_like(poses)
         ms = _timed(lambda: A.minimise(wl, poses, cfg.steps, launch=shp, pose_out=out, scratch=scratch), 5)
-        e = {"workload": names[idx], "poses": wl.n_poses, "adam_steps": cfg.steps, "value": round(wl.n_poses / ms * 1e3, 1),
-             "unit": UNIT, "ms": round(ms, 3), "launch": {"lanes_per_pose": shp.lanes_per_pose},
+        e = {"workload": names[key], "poses": wl.n_poses, "adam_steps": cfg.steps,
+             "value": round(wl.n_poses / ms * 1e3, 1), "unit": UNIT, "ms": round(ms, 3),
+             "launch": {"lanes_per_pose": shp.lanes_per_pose},
              "roofline_frac": round(algorithmic_bytes(stats) / (ms / 1e3) / 1e9 / _peak(), 4),
-             "list_entries_per_lookup": round(float(stats[2]) / max(float(stats[1]), 1.0), 2)}
+             "list_entries_per_lookup": round(float(stats[2]) / max(float(stats[1]), 1.0), 2),
+             "list_entries_per_s": round(float(stats[2]) / (ms / 1e3), 1)}
         if idx == 2:
             # list lengths seen by the starting poses' beads (the workload's "0-80 entries")
             xyz = np.asarray(cfg.ligands[0][0])
@@ -264,9 +279,13 @@ def other_configs(args, device, shape):
             vox = (near[..., 0] * ng.dim[1] + near[..., 1]) * ng.dim[2] + near[..., 2]
             cnt = np.where(inn, hdr[np.clip(vox, 0, len(hdr) - 1), 1], 0)
             e["bead_fraction_with_lists"] = round(float((cnt > 0).mean()), 3)
-            e["list_length_hist"] = np.bincount(np.minimum(cnt[cnt > 0], 80), minlength=81).tolist()
+            edges = [0, 1, 6, 11, 21, 41, 81, 1 << 30]
+            h = np.histogram(cnt, bins=edges)[0]
+            e["list_length_hist"] = {f"{lo}-{hi - 1}" if hi < 1 << 30 else f">={lo}": int(c)
+                                     for lo, hi, c in zip(edges[:-1], edges[1:], h)}
+            e["list_length_p50_p90_p99"] = [int(x) for x in np.percentile(cnt[cnt > 0], [50, 90, 99])]
             e["list_length_max"] = int(cnt.max())
-        res[f"config{idx}"] = e
+        res[key] = e
         del grid, wl, scratch
         torch.cuda.empty_cache()
     cfg = synth.make_config(3, seed=0, scale=args.scale)
@@ -385,6 +404,28 @@ def serving_run(args, device):
     del grids
     torch.cuda.empty_cache()
     return out
+
+
+def summary(out):
+    """The headline figures of the line in a few hundred bytes."""
+    r = lambda x, n=1: None if x is None else round(float(x), n)
+    sm = {"batched_poses_per_s": out["value"], "e2e_poses_per_s": out["e2e"]["value"],
+          "roofline_frac": out["roofline"]["frac"]}
+    if "plain" in out:
+        sm["plain_poses_per_s"] = out["plain"]["value"]
+        sm["batched_vs_plain"] = out["batched_vs_plain"]
+    if "cpu_baseline" in out:
+        sm["cpu_baseline_poses_per_s"] = r(out["cpu_baseline"]["value"], 2)
+    for k, v in out.get("configs", {}).items():
+        sm[f"{k}_value"] = v.get("value", (v.get("fused") or {}).get("value"))
+        if "bead_fraction_with_lists" in v:
+            sm[f"{k}_bead_fraction_with_lists"] = v["bead_fraction_with_lists"]
+            sm[f"{k}_list_length_max"] = v["list_length_max"]
+    for i, run in enumerate(out.get("serving", {}).get("runs", [])):
+        sm[f"serving{i}"] = {"rate": run.get("arrival_rate_per_s"), "poses_per_s": r(run.get("poses_per_s")),
+                             "p50_s": r(run.get("p50_s"), 3), "p99_s": r(run.get("p99_s"), 3),
+                             "backlog_requests": run.get("backlog_requests")}
+    return sm
 
 
 # --------------------------------------------------------------------------- ours
@@ -519,7 +560,47 @@ def run_ours(args):
             out["serving"] = serving_run(args, device)
     replicas.finish(R)
     if rank == 0:
+        out["summary"] = summary(out)  # last: the headline figures survive a truncated tail of the line
         print(json.dumps(out), flush=True)
+
+
+# --------------------------------------------------------------------------- profiler case
+def run_profile_case(args):
+    """The minimiser alone on one configuration, launched ``--launches`` times
+    (the case the committed ncu summaries capture).  ``--types`` shrinks the
+    number of ligand types, and so the grid, to keep captures small; prints
+    one JSON line with the mean time of the launches after the first."""
+    import torch
+
+    import attract_b200 as A
+    from attract_b200 import synth
+
+    A.load_library()
+    cfg = synth.make_config(args.config, seed=0, scale=args.scale, n_types=args.types, clustered=args.clustered)
+    steps = cfg.steps if args.adam_steps < 0 else args.adam_steps
+    grid = A.Grid.build(cfg.rec_xyz, cfg.rec_type, cfg.ff, cfg.geom, cutoff=cfg.cutoff, nb_refine=args.refine)
+    ligs = A.LigandSet(cfg.ligands)
+    order = sorted(range(len(cfg.ligands)), key=lambda i: -len(cfg.ligands[i][0]))
+    lanes = args.lanes or 32
+    wl = A.Workload([grid], ligs, [A.Segment(0, i, len(cfg.poses[i])) for i in order], lanes_per_pose=lanes)
+    poses = torch.tensor(np.concatenate([cfg.poses[i] for i in order]).astype(np.float32), device="cuda")
+    shape = A.LaunchShape(lanes, args.threads or 128)
+    scratch = A.MinimiseScratch(wl.n_poses, wl.device)
+    out = torch.empty_like(poses)
+    times = []
+    for _ in range(args.launches):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        A.minimise(wl, poses, steps, pose_out=out, launch=shape, scratch=scratch)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    _, _, _, st = A.minimise(wl, poses, steps, launch=shape, stats=True)
+    st = st.cpu().numpy().tolist()
+    ms = float(np.mean(times[1:])) if len(times) > 1 else times[0]
+    print(json.dumps({"config": args.config, "clustered": args.clustered, "scale": args.scale, "types": args.types,
+                      "poses": wl.n_poses, "steps": steps, "lanes": lanes, "threads": shape.block_threads, "ms": ms,
+                      "poses_per_s": wl.n_poses / ms * 1e3, "stats": st, "brick_gb": grid.bricks.numel() * 4 / 1e9}))
 
 
 # --------------------------------------------------------------------------- reference
@@ -536,7 +617,9 @@ def run_reference(args):
 
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.profile_case:
+        run_profile_case(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

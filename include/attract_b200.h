@@ -58,6 +58,9 @@ extern "C" {
 /* device-wide kernel error word (att_kernel_status) */
 #define ATT_KERR_COPY_TIMEOUT 1 /* a warp gave up waiting for its grid-brick / record bulk copies and returned */
 #define ATT_KERR_BOUNDS 2       /* (ATT_BOUNDS_CHECK builds) an index failed its check; the access was skipped */
+#define ATT_KERR_BAD_SEGMENT 4  /* a segment named a missing grid or ligand or reached beyond n_pose_rows, or a
+                                   pose's conformer index (pose_lig) or its ligand's bead range left the ligand
+                                   set: those poses were skipped (outputs unwritten), checked before any access */
 
 /* A pose is served by lanes_per_pose lanes holding up to 8 beads each; a
    ligand with more than 8 * lanes_per_pose beads is evaluated in chunks of that
@@ -117,6 +120,8 @@ typedef struct AttLigands {
   const int* offset;    /* [n_lig + 1] first bead of each ligand */
   int n_lig;
   int max_beads;        /* max over ligands of offset[l+1]-offset[l] */
+  int n_beads;          /* rows of beads; a ligand whose offsets leave [0, n_beads] is skipped */
+  int pad_;
 } AttLigands;
 
 /* A run of consecutive poses scored against one grid with one ligand. */
@@ -185,12 +190,22 @@ long long att_grid_brick_bytes(const AttGridGeom* geom, int with_outer);
 int att_grid_repack(const AttGridGeom* geom, const float* inner_dev, const float* outer_dev,
                     void* bricks_dev, void* stream);
 
-/* One energy (+gradient) evaluation of every pose of every segment.
+/* Arguments shared by the scoring entry points below: segs_dev [n_segs] and
+   seg_tile_dev [n_segs+1] (first work tile of each segment; a tile is
+   32/lanes_per_pose consecutive poses of one segment) on the device;
+   n_pose_rows = B, the rows of the pose and per-pose output arrays.  The
+   kernels check every segment (grid < n_grids, lig < ligs->n_lig, pose0 >= 0,
+   pose0 + n_poses <= B), every conformer index (pose_lig) and every ligand's
+   bead range (within ligs->n_beads, at most ligs->max_beads beads) before any
+   access; a pose that fails is skipped, its outputs stay unwritten, and
+   ATT_KERR_BAD_SEGMENT is set in the device error word (att_kernel_status).
+
+   One energy (+gradient) evaluation of every pose of every segment.
    pose_dev [B][6] (or [B][16]); pose_lig_dev [B] optional per-pose ligand offset (conformers);
    energy_dev [B]; grad_dev [B][6] (Euler) or [B][16] dE/dmat (pose_format 1), may be NULL;
    status_dev [B] optional.  test5.py:404-429. */
 int att_energrad(const AttGrid* grids, int n_grids, const AttLigands* ligs,
-                 const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
+                 const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles, int n_pose_rows,
                  const float* pose_dev, const int* pose_lig_dev, const AttEvalCfg* cfg,
                  float* energy_dev, float* grad_dev, int* status_dev,
                  const AttLaunchCfg* launch, void* stream);
@@ -205,7 +220,7 @@ int att_energrad(const AttGrid* grids, int n_grids, const AttLigands* ligs,
    seg_tile_dev [n_segs+1]: first work tile of each segment (a tile is
    32/lanes_per_pose consecutive poses of one segment).  test5.py:436-467. */
 int att_minimise(const AttGrid* grids, int n_grids, const AttLigands* ligs,
-                 const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
+                 const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles, int n_pose_rows,
                  const float* pose_in_dev, float* pose_out_dev, const int* pose_lig_dev,
                  float* adam_state_dev, const AttAdamCfg* cfg, int steps,
                  float* energy_dev, int* status_dev, int* work_counter_dev,
@@ -222,7 +237,7 @@ int att_minimise(const AttGrid* grids, int n_grids, const AttLigands* ligs,
    reports it (test5.py:465).  A step with a non-finite gradient is skipped and
    flagged in status_dev.  work_counter_dev: one int of scratch. */
 int att_minimise_schema(const AttGrid* grids, int n_grids, const AttLigands* ligs,
-                        const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
+                        const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles, int n_pose_rows,
                         const float* pose_in_dev, float* pose_out_dev, const int* pose_lig_dev,
                         const AttSchemaCfg* cfg, float* energy_dev, int* status_dev, int* work_counter_dev,
                         const AttLaunchCfg* launch, void* stream);
@@ -232,7 +247,7 @@ int att_minimise_schema(const AttGrid* grids, int n_grids, const AttLigands* lig
    float [n_types][dim..][4] (channel 0 receives the gradient; the caller zeroes
    the buffers).  Recomputes the forward instead of storing per-bead weights. */
 int att_energrad_backward(const AttGrid* grids, int n_grids, const AttLigands* ligs,
-                          const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles,
+                          const AttSegment* segs_dev, int n_segs, const int* seg_tile_dev, int n_tiles, int n_pose_rows,
                           const float* pose_dev, const int* pose_lig_dev, const AttEvalCfg* cfg,
                           const float* dL_dE_dev, float* dL_dpose_dev,
                           float* dgrid_inner_dev, float* dgrid_outer_dev,
@@ -252,7 +267,13 @@ int att_build_potential_grid(const AttGridGeom* geom, const float* rec_dev, int 
    ascending bead index.  att_nbgrid_count writes hdr_dev [V][2] = {start, count}
    and the entry total (one u64 on the device); it needs
    att_nbgrid_workspace_bytes(V) bytes of scratch.  att_nbgrid_fill then writes
-   the entries.  test-calc-grid-energy.py:90-103. */
+   the entries.  The starts are 32-bit: a total above 2^32 - 1 (the u64 at
+   total_dev holds the true count) means they wrapped, and the caller must not
+   fill or use the lists.  A point is within the radius when
+   fl(fl(fl(dx*dx) + fl(dy*dy)) + fl(dz*dz)) <= fl(radius*radius), each float32
+   operation rounded on its own (dx = fl(x - rx), x = fl(origin + fl(i*spacing))),
+   so a host restatement reproduces the lists bit for bit.
+   test-calc-grid-energy.py:90-103. */
 long long att_nbgrid_workspace_bytes(long long n_voxels);
 int att_nbgrid_count(const AttGridGeom* geom, const float* rec_dev, int n_rec, float radius,
                      uint32_t* hdr_dev, unsigned long long* total_dev, void* workspace_dev,

@@ -292,8 +292,11 @@ def nb_energrad(pos, ltype, geom, nb_hdr, nb_list, rec, rtype, pair, mode="refer
     ``[n_voxels, 2]`` (start, count) into ``nb_list``; ``geom["nb_refine"]`` = r
     > 1 puts the lists on the inner grid refined r times per axis (an
     extension: lists within plateau + the refined half-diagonal find the same
-    pairs with fewer entries).  ``absolute=True`` sums
-    |term| instead of term (magnitude scales for float32 tolerances).
+    pairs with fewer entries).  ``absolute=True`` sums the magnitudes of
+    every additive component of each term instead of the term -- |rc/d^8| +
+    |ac/d^6| + |emin term| + |plateau energy| for the energy, and likewise
+    for the gradient -- the scale against which float32 rounding of the
+    term is bounded (the components cancel near the potential's zero).
     """
     dt = np.dtype(dtype)
     pos = np.asarray(pos, dt)
@@ -343,7 +346,17 @@ def nb_energrad(pos, ltype, geom, nb_hdr, nb_list, rec, rtype, pair, mode="refer
         gfac = dt.type(2) * gmain
     gv = gfac[:, None] * d
     if absolute:
-        e, gv = np.abs(e), np.abs(gv)
+        dc = np.maximum(dsq, rcap2)
+        rr2 = 1.0 / dc
+        rr6 = rr2 ** 3
+        near = dc < rmin2
+        wiv = np.where(near, 1.0, np.abs(ivor))
+        e = wiv * (np.abs(rc) * rr6 * rr2 + np.abs(ac) * rr6) + np.where(near, np.abs((ivor - 1.0) * emin), 0.0) \
+            + np.abs(eplat)
+        gm = np.where(dsq < rcap2, 0.0, wiv * rr2 ** 4 * (3.0 * np.abs(ac) + 4.0 * np.abs(rc) * rr2))
+        if mode == "reference":
+            gm = gm + np.abs(gplat) * p / np.sqrt(dsq)
+        gv = 2.0 * gm[:, None] * np.abs(d)
     np.add.at(E, bead, e)
     np.add.at(G, bead, gv)
     return E.reshape(shp), G.reshape(shp + (3,))
@@ -650,6 +663,46 @@ def build_nbgrid(rec, geom, radius):
     flat = np.concatenate([np.sort(np.asarray(x, np.int64)) for x in lists]) if cnt.sum() else np.zeros(0, np.int64)
     hdr = np.stack([start, cnt], 1).astype(np.uint32)
     return hdr, flat.astype(np.uint16)
+
+
+def build_nbgrid_f32(rec32, origin32, spacing32, dim, radius32):
+    """Neighbour lists with the builder kernel's float32 arithmetic, bit for bit.
+
+    The same membership rule as :func:`build_nbgrid` (receptor beads within
+    ``radius`` of grid point origin + i*s, test-calc-grid-energy.py:90-103),
+    computed as the GPU builder computes it: the point as
+    ``fl(origin + fl(i * s))``, the squared distance as
+    ``fl(fl(fl(dx*dx) + fl(dy*dy)) + fl(dz*dz))`` with ``dx = fl(x - r_x)``, and
+    the test ``d2 <= fl(radius * radius)``, every operation rounded to float32
+    on its own.  ``rec32`` [R, 3] float32 in the order the lists index; the
+    entries of a point are in ascending index order.  A float64 KD-tree query
+    with a margin picks the candidates; the float32 test decides.
+    """
+    from scipy.spatial import cKDTree
+
+    f = np.float32
+    rec32 = np.asarray(rec32, f).reshape(-1, 3)
+    o = np.asarray(origin32, f).reshape(3)
+    s = f(spacing32)
+    r2 = f(radius32) * f(radius32)
+    dim = [int(d) for d in dim]
+    ax = [o[k] + np.arange(dim[k], dtype=f) * s for k in range(3)]  # each a rounded product, then sum
+    pts = np.stack(np.meshgrid(*ax, indexing="ij"), -1).reshape(-1, 3)
+    tree = cKDTree(rec32.astype(np.float64))
+    cand = tree.query_ball_point(pts.astype(np.float64), float(np.sqrt(np.float64(r2))) + 1e-3)
+    cnt = np.array([len(x) for x in cand], np.int64)
+    gi = np.repeat(np.arange(len(pts)), cnt)
+    rj = np.concatenate([np.asarray(x, np.int64) for x in cand]) if cnt.sum() else np.zeros(0, np.int64)
+    d = pts[gi] - rec32[rj]  # float32, rounded per component
+    dsq = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+    keep = dsq <= r2
+    gi, rj = gi[keep], rj[keep]
+    order = np.lexsort((rj, gi))
+    gi, rj = gi[order], rj[order]
+    n = np.bincount(gi, minlength=len(pts)).astype(np.int64)
+    start = np.cumsum(n) - n
+    hdr = np.stack([start, n], 1).astype(np.uint32)
+    return hdr, rj.astype(np.uint16)
 
 
 def repack_bricks(inner, outer):

@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden from the reference's own data.
 
-Run once in a checkout that has the reference mounted (default path below);
-the GPU box and the test suite only read the committed ``.npz`` outputs.
+Run once where a checkout of the reference exists, giving its path; the GPU
+box and the test suite only read the committed ``.npz`` outputs.
 
-    python tests/golden/make_golden.py [/path/to/attract-jax]
+    python tests/golden/make_golden.py /path/to/attract-jax
 
 Sources (all from sjdv1982/attract-jax):
 * energy-init/make-energy-init.out + energy-init/score.out: 296 single-pair
@@ -108,4 +108,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of the attract-jax checkout>")
+    main(sys.argv[1])

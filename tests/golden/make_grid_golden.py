@@ -8,7 +8,7 @@ imported from the reference checkout, which needs only NumPy), checks that the
 reference reads back what was written, and stores the bytes and the reference
 reader's arrays in attract_grid_golden.npz.
 
-    python tests/golden/make_grid_golden.py [/path/to/reference]
+    python tests/golden/make_grid_golden.py /path/to/attract-jax
 """
 import os
 import sys
@@ -69,4 +69,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of the attract-jax checkout>")
+    main(sys.argv[1])

@@ -1,11 +1,35 @@
-"""Seeded small cases shared by the GPU parity tests: grids, ligands and poses
+"""Seeded small cases shared by the GPU parity tests (grids, ligands and poses
 that exercise the inner grid, the outer grid, the space outside both, the
-neighbour lists and the pair-table branches."""
+neighbour lists and the pair-table branches) and the north-star tolerance
+check every parity test reports.
+
+The north-star tolerance: per-pose energies within 1e-5 relative (or 1e-4
+kcal/mol absolute) of the float64 oracle, gradients within 1e-4 relative
+(rotation and translation parts separately, each with a floor of 1e-5 that
+only binds for gradients below 0.1).  A pose outside it must lie within a
+counted float32 bound (``float32_bounds``):
+
+* arithmetic: 32 u times the sum of the magnitudes of every additive
+  component of every term (grid corners; r^-8, r^-6 and plateau parts of the
+  pair terms), u = 2^-24 (about 8 rounding steps per term: an approximate
+  reciprocal of 1 ulp raised to the 8th power, products and the lane and
+  shuffle-tree sums);
+* inputs: the float32 bead positions, off by up to delta = 8 u (|x| + |X| +
+  |X - o|) (rotation from float32 sines, the product with the ligand frame,
+  the translation and the grid-frame shift): the spread of each bead's
+  float64 energy and gradient over +-2 delta along each axis, which covers
+  the slope and any jump within reach (a cell face of the analytic gradient,
+  the energy cap, the inner/outer grid boundary).
+"""
 from __future__ import annotations
 
 import numpy as np
 
 import attract_oracle as O
+
+U = 2.0 ** -24
+NS_E_REL, NS_E_ABS, NS_G_REL = 1e-5, 1e-4, 1e-4
+G_FLOOR = 1e-5  # kcal/mol/A (/rad): only binds for gradients below 0.1
 
 
 def small_case(seed=0, n_types=4, n_rtypes=3, n_rec=60, n_lig_beads=9, n_poses=64, cap=True, ivor_mix=False,
@@ -96,3 +120,71 @@ def oracle_scales(case, poses, mode="reference", quirk=True, position_term=False
         es = es + 0.2 * (gabs * (1 + np.linalg.norm(X, axis=2))).sum(1)
     gs = (gabs * (1 + np.linalg.norm(r, axis=2))).sum(1)
     return es, gs
+
+
+def float32_bounds(poses, lig, gt, lt, G, mode):
+    """Per-pose (energy, rotation-gradient, translation-gradient) float32 bounds."""
+    X = O.transform(poses, lig)                                     # [B, N, 3]
+    t = poses[:, None, 3:6]
+    ab = lambda a: None if a is None else np.abs(a)
+    Eg, gg = O.grid_energrad(X, gt, G["geom"], ab(G.get("inner")), ab(G.get("outer")), True, "reference")
+    En, gn = O.nb_energrad(X, lt, G["geom"], G.get("nb_hdr"), G.get("nb_list"), G["rec"], G["rtype"], G["pair"],
+                           mode, absolute=True)
+    if mode == "analytic":
+        gg = np.repeat(Eg[..., None], 3, -1) * 2.0 / G["geom"]["spacing"]
+    S_e = Eg + En                                                   # [B, N]
+    S_g = np.linalg.norm(np.abs(gg) + gn, axis=-1)                  # [B, N]
+    o = np.asarray(G["geom"]["origin"])
+    delta = 8 * U * (np.linalg.norm(lig, axis=-1)[None] + np.linalg.norm(X, axis=-1) + np.linalg.norm(X - o, axis=-1))
+    # the bead terms' spread over the float32 position uncertainty, probed
+    # along each axis at +-2 delta: the slope in smooth regions, and any jump
+    # within reach (an analytic-gradient cell face, the energy cap, the
+    # inner/outer grid boundary) that float32 positions may land across
+    _, gb = O.bead_energrad(X, gt, lt, G, mode)
+    sE = np.zeros(X.shape[:2])
+    sG = np.zeros(X.shape[:2])
+    for k in range(3):
+        d = np.zeros(X.shape)
+        d[..., k] = 2 * delta
+        Ep, gp = O.bead_energrad(X + d, gt, lt, G, mode)
+        Em, gm = O.bead_energrad(X - d, gt, lt, G, mode)
+        sE = np.maximum(sE, np.abs(Ep - Em))
+        sG = np.maximum(sG, np.linalg.norm(gp - gm, axis=-1))
+    arm = 1.0 + np.linalg.norm(X - t, axis=-1)
+    gnorm = np.linalg.norm(gb, axis=-1)
+    bE = 32 * U * S_e.sum(1) + sE.sum(1)
+    bT = 32 * U * S_g.sum(1) + sG.sum(1)
+    bR = 2.0 * (32 * U * (S_g * arm).sum(1) + (sG * arm + gnorm * delta).sum(1))
+    return bE, bR, bT
+
+
+def north_star_report(name, E, G, Eo, Go, bounds):
+    """Fractions within the north-star tolerance; asserts the rest lie within
+    the float32 bounds.  Returns the report dict (also printed)."""
+    bE, bR, bT = bounds
+    dE = np.abs(E - Eo)
+    tolE = np.maximum(NS_E_REL * np.abs(Eo), NS_E_ABS)
+    inE = dE <= tolE
+    out = {"poses": len(E), "energy_within_1e-5": float(inE.mean())}
+    ok = inE | (dE <= bE)
+    worst = {"energy": float((dE / np.maximum(tolE, bE)).max())}
+    if G is not None:  # rotation part: every column but the last three (Euler angles or the 3x3 block)
+        G, Go = G.reshape(len(G), -1), Go.reshape(len(Go), -1)
+        dR = np.linalg.norm(G[:, :-3] - Go[:, :-3], axis=1)
+        dT = np.linalg.norm(G[:, -3:] - Go[:, -3:], axis=1)
+        tolR = NS_G_REL * np.linalg.norm(Go[:, :-3], axis=1) + G_FLOOR
+        tolT = NS_G_REL * np.linalg.norm(Go[:, -3:], axis=1) + G_FLOOR
+        inG = (dR <= tolR) & (dT <= tolT)
+        out["gradient_within_1e-4"] = float(inG.mean())
+        out["both_within"] = float((inE & inG).mean())
+        ok &= ((dR <= tolR) | (dR <= bR)) & ((dT <= tolT) | (dT <= bT))
+        worst["rotation"] = float((dR / np.maximum(tolR, bR)).max())
+        worst["translation"] = float((dT / np.maximum(tolT, bT)).max())
+        out["outside_explained_by_float32_bound"] = int(((~(inE & inG)) & ok).sum())
+    else:
+        out["outside_explained_by_float32_bound"] = int(((~inE) & ok).sum())
+    out["max_error_over_allowed"] = worst
+    out["unexplained"] = int((~ok).sum())
+    print(f"\n[north-star] {name}: {out}")
+    assert out["unexplained"] == 0, (name, out, np.flatnonzero(~ok)[:10])
+    return out

@@ -163,3 +163,20 @@ def test_grid_scatter_equals_a_deterministic_host_sum():
     E1, G1, _ = A.energrad(wl, P)
     E2, G2, _ = A.energrad(wl, P)
     assert torch.equal(E1, E2) and torch.equal(G1, G2)
+
+
+def test_backward_refuses_bricks_repacked_after_its_forward():
+    """The backward recomputes its forward from the bricks: if another forward
+    repacked them from edited dense grids in between, it raises instead of
+    returning gradients of the new grid."""
+    A, docking_energy, c, grid, wl = _setup(seed=35)
+    grid.inner.requires_grad_(True)
+    P = torch.tensor(c["poses"], dtype=torch.float32, device="cuda", requires_grad=True)
+    E0 = docking_energy(wl, P)
+    with torch.no_grad():
+        grid.inner[..., 0] += 0.5
+    E1 = docking_energy(wl, P)  # repacks
+    with pytest.raises(RuntimeError, match="repacked"):
+        E0.backward()
+    E1.backward()  # the latest forward still differentiates
+    assert torch.isfinite(P.grad).all()

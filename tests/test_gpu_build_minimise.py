@@ -41,21 +41,42 @@ def test_potential_grid_builder_vs_oracle():
         assert bad.mean() < 1e-4, bad.mean()
 
 
+def _device_lists(g):
+    """The grid's neighbour lists as the kernels read them (receptor beads
+    named by device position) and the device-order float32 receptor."""
+    hdr = g.nb_hdr.cpu().numpy().view(np.uint32)
+    lst = g.nb_list.cpu().numpy().view(np.uint16)
+    rec = g.rec.cpu().numpy()[: g.n_rec, :3]
+    return hdr, lst, rec
+
+
+def _f32_lists(g, rec32, radius):
+    c = g.nb_geom.to_c()
+    return O.build_nbgrid_f32(rec32, np.array(c.origin[:], np.float32), c.spacing, c.dim[:], np.float32(radius))
+
+
 def test_nbgrid_builder_vs_oracle():
+    """Neighbour lists are index work: the GPU builder's lists equal, bit for
+    bit, the oracle's float32 restatement of the same membership test; and
+    that restatement differs from the float64 lists only for pairs within
+    float32 rounding of the radius."""
     A, ff, geom, xyz, t = _small_receptor(seed=1)
     radius = 3.0 + np.sqrt(3) / 2 + 0.01
     g = A.Grid.build(xyz, t, ff, geom, list_radius=radius, potentials=False, nb_refine=1)
-    _, _, hdr, lst = g.dense_host()
-    ref_hdr, ref_lst = O.build_nbgrid(xyz, geom.as_dict(), radius)
-    assert np.array_equal(hdr[:, 0], np.cumsum(hdr[:, 1]) - hdr[:, 1])  # CSR starts
-    if not (np.array_equal(hdr, ref_hdr) and np.array_equal(lst[: len(ref_lst)], ref_lst)):
-        # only pairs within float32 rounding of the radius may differ
+    hdr, lst, rec32 = _device_lists(g)
+    ref_hdr, ref_lst = _f32_lists(g, rec32, radius)
+    assert np.array_equal(hdr, ref_hdr)
+    assert np.array_equal(lst[: len(ref_lst)], ref_lst)
+    # the float32 test against the exact one (caller order, float64)
+    _, _, h64, l64 = g.dense_host()
+    ref_hdr64, ref_lst64 = O.build_nbgrid(xyz, geom.as_dict(), radius)
+    if not (np.array_equal(h64, ref_hdr64) and np.array_equal(l64[: len(ref_lst64)], ref_lst64)):
         pts = O.grid_points(geom.as_dict()).reshape(-1, 3)
         d = np.linalg.norm(pts[:, None, :] - xyz[None], axis=2)
         got = np.zeros_like(d, dtype=bool)
-        for v in range(len(hdr)):
-            s, n = hdr[v]
-            got[v, lst[s:s + n]] = True
+        for v in range(len(h64)):
+            s0, n = h64[v]
+            got[v, l64[s0:s0 + n]] = True
         mismatch = got != (d <= radius)
         assert np.all(np.abs(d[mismatch] - radius) < 1e-4)
 
@@ -71,11 +92,14 @@ def test_refined_list_grid_finds_the_same_pairs(refine):
     gr = A.Grid.build(xyz, t, ff, geom, cutoff=6.0, nb_refine=refine)
     fine = geom.refined(refine)
     radius = geom.plateau + fine.spacing * np.sqrt(3) / 2 + 1e-3
+    dh, dl, rec32 = _device_lists(gr)
+    ref_dh, ref_dl = _f32_lists(gr, rec32, radius)
+    assert np.array_equal(dh, ref_dh) and np.array_equal(dl[: len(ref_dl)], ref_dl)  # bit-exact
     _, _, hdr, lst = gr.dense_host()
     ref_hdr, ref_lst = O.build_nbgrid(xyz, fine.as_dict(), radius)
     assert hdr.shape == ref_hdr.shape
     pts = O.grid_points(fine.as_dict()).reshape(-1, 3)
-    for v in np.flatnonzero(hdr[:, 1] != ref_hdr[:, 1]):  # only float32 rounding at the radius
+    for v in np.flatnonzero(hdr[:, 1] != ref_hdr[:, 1]):  # float64 vs float32: only rounding at the radius
         d = np.linalg.norm(pts[v] - xyz, axis=1)
         got = set(lst[hdr[v, 0]:hdr[v, 0] + hdr[v, 1]].tolist())
         want = set(np.flatnonzero(d <= radius).tolist())

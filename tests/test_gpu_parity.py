@@ -1,12 +1,13 @@
 """CUDA path (through the C ABI) against the oracle on identical inputs.
 
-Tolerances (float32 kernels vs the float64 oracle):
-* energy per pose: |dE| <= 1e-5 * S_E + 1e-4 kcal/mol, S_E = sum of |term| over
-  every grid corner and pair term (float32 summation error is bounded relative
-  to the sum of magnitudes, not to a total in which terms cancel); for the
-  realistic cases S_E is within 3 % of |E|, so this is ~1e-5 relative;
-* gradient per pose and component: |dg| <= 1e-4 * S_g + 1e-3, S_g = sum of
-  |gradient term| (1 + |r_b|) (torques carry the lever arm r_b).
+Every comparison with the float64 oracle reports the north-star metric --
+the fraction of poses whose energy is within 1e-5 relative (or 1e-4
+kcal/mol absolute) and whose gradient is within 1e-4 relative -- and asserts
+that every pose outside it lies within the counted float32 bound of
+``gpu_cases.float32_bounds`` (arithmetic: 32 u times the summed magnitudes of
+every term component; inputs: the spread of each bead's terms over its
+float32 position uncertainty).  The checks against ATTRACT's and JAX's own
+outputs at the end use those files' printed precision.
 """
 import numpy as np
 import pytest
@@ -14,7 +15,7 @@ import torch
 
 import attract_oracle as O
 from conftest import dat_poses, mono_leu_setup
-from gpu_cases import oracle_scales, small_case, to_device_grid
+from gpu_cases import float32_bounds, north_star_report, small_case, to_device_grid
 
 pytestmark = pytest.mark.gpu
 
@@ -31,13 +32,15 @@ def _wl(A, grid, lig, gt, lt, n, lanes=8):
     return A.Workload([grid], ligs, [A.Segment(0, 0, n)], lanes_per_pose=lanes)
 
 
-def _check(E, G, Eo, Go, es, gs):
-    dE = np.abs(E - Eo)
-    assert np.all(dE <= 1e-5 * es + 1e-4), (dE.max(), np.argmax(dE - 1e-5 * es))
-    if G is not None:
-        dG = np.abs(G - Go)
-        tol = 1e-4 * gs[:, None] + 1e-3
-        assert np.all(dG <= tol), (dG.max(), np.unravel_index(np.argmax(dG - tol), dG.shape))
+def _check(name, c, E, G, Eo, Go, mode="reference", gravity=0.0, poses=None):
+    """North-star report of kernel vs float64 oracle on case ``c``."""
+    poses = c["poses"] if poses is None else poses
+    bE, bR, bT = float32_bounds(poses, c["lig"], c["gt"], c["lt"], c["G"], mode)
+    if gravity:  # gravity * |t|^2 and its gradient: a few roundings of their size
+        t2 = (poses[:, 3:] ** 2).sum(1)
+        bE = bE + 8 * 2.0 ** -24 * gravity * t2
+        bT = bT + 8 * 2.0 ** -24 * 2 * gravity * np.sqrt(t2)
+    return north_star_report(name, E, G, Eo, Go, (bE, bR, bT))
 
 
 @pytest.mark.parametrize("mode", ["reference", "analytic"])
@@ -51,15 +54,14 @@ def test_energrad_small_grid(mode, lanes):
     E, G, S = A.energrad(wl, poses, A.EvalOptions(grad_mode=mode))
     torch.cuda.synchronize()
     Eo, Go = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], c["G"], mode=mode)
-    es, gs = oracle_scales(c, c["poses"], mode)
-    _check(E.cpu().numpy(), G.cpu().numpy(), Eo, Go, es, gs)
+    _check(f"small grid, {mode}, {lanes} lanes", c, E.cpu().numpy(), G.cpu().numpy(), Eo, Go, mode)
     assert np.all(S.cpu().numpy() == 0)
 
 
 def test_energrad_branches_ivor_nocap_gravity():
     """Uncapped potentials with repulsive (ivor=-1) pairs: clashes reach 1e10
-    kcal/mol, where float32 position rounding dominates; the bound adds it and
-    the gradient bound is five times the float32 oracle's own deviation."""
+    kcal/mol, where float32 position rounding dominates (the bound's input
+    term), plus gravity."""
     A = _engine()
     c = small_case(seed=2, n_poses=64, cap=False, ivor_mix=True)
     grid = to_device_grid(c)
@@ -67,13 +69,7 @@ def test_energrad_branches_ivor_nocap_gravity():
     poses = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
     E, G, _ = A.energrad(wl, poses, A.EvalOptions(gravity=0.1))
     Eo, Go = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], c["G"], gravity=0.1)
-    _, G32 = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], c["G"], gravity=0.1, dtype=np.float32)
-    es, gs = oracle_scales(c, c["poses"], position_term=True)
-    t = c["poses"][:, 3:]
-    es = es + 0.1 * (t * t).sum(1)
-    _check(E.cpu().numpy(), None, Eo, None, es, gs)
-    dG = np.abs(G.cpu().numpy() - Go)
-    assert np.all(dG <= 5 * np.abs(G32 - Go) + 1e-4 * gs[:, None] + 1e-3)
+    _check("uncapped, ivor +-1, gravity", c, E.cpu().numpy(), G.cpu().numpy(), Eo, Go, gravity=0.1)
 
 
 @pytest.mark.parametrize("n_beads,lanes", [(30, 32), (60, 32), (60, 16), (60, 8)])
@@ -89,8 +85,7 @@ def test_dense_lists_many_pair_windows(n_beads, lanes):
     poses = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
     E, G, S = A.energrad(wl, poses)
     Eo, Go = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], c["G"])
-    es, gs = oracle_scales(c, c["poses"])
-    _check(E.cpu().numpy(), G.cpu().numpy(), Eo, Go, es, gs)
+    _check(f"dense lists, {n_beads} beads, {lanes} lanes", c, E.cpu().numpy(), G.cpu().numpy(), Eo, Go)
     # the case does reach many windows: entries per pose far above a team's buffer
     hdr = c["G"]["nb_hdr"]
     assert hdr[:, 1].max() > 64
@@ -122,8 +117,7 @@ def test_energrad_partial_grids(what):
     poses = torch.tensor(c["poses"], dtype=torch.float32, device="cuda")
     E, G, _ = A.energrad(wl, poses)
     Eo, Go = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], c["G"])
-    es, gs = oracle_scales(c, c["poses"])
-    _check(E.cpu().numpy(), G.cpu().numpy(), Eo, Go, es, gs)
+    _check(f"partial grids: {what}", c, E.cpu().numpy(), G.cpu().numpy(), Eo, Go)
 
 
 def test_trilinear_quirk_integer_voxels():
@@ -159,10 +153,12 @@ def test_mat_pose_format_and_consistency():
     mats = O.pose_to_mat(c["poses"])
     E, dM, _ = A.energrad(wl, torch.tensor(mats, dtype=torch.float32, device="cuda"))
     Eo, dMo = O.energrad_mat(mats, c["lig"], c["gt"], c["lt"], c["G"])
-    es, gs = oracle_scales(c, c["poses"])
-    assert np.all(np.abs(E.cpu().numpy() - Eo) <= 1e-5 * es + 1e-4)
-    d = np.abs(dM.cpu().numpy() - dMo).reshape(32, -1)
-    assert np.all(d <= 1e-4 * gs[:, None] + 1e-3)
+    # dE/dmat: the 3x3 block (ligand-frame lever arms) and the translation row
+    dM = dM.cpu().numpy()
+    got = np.concatenate([dM[:, :3, :3].reshape(32, 9), dM[:, 3, :3]], 1)
+    ref = np.concatenate([dMo[:, :3, :3].reshape(32, 9), dMo[:, 3, :3]], 1)
+    _check("4x4 pose input, dE/dmat", c, E.cpu().numpy(), got, Eo, ref)
+    assert np.all(dM[:, :, 3] == 0)
 
 
 def test_edge_cases_empty_outside_nan():

@@ -66,7 +66,7 @@ def test_error_path_without_gpu():
     from attract_b200 import _lib
 
     lib = _lib.load(_lib_path())
-    rc = lib.att_energrad(None, 0, None, None, 0, None, 0, None, None, None, None, None, None, None, None)
+    rc = lib.att_energrad(None, 0, None, None, 0, None, 0, 0, None, None, None, None, None, None, None, None)
     assert rc == 1
     assert b"n_grids" in lib.att_last_error_string()
     g = _lib.AttGridGeom()
@@ -176,3 +176,42 @@ def test_attract_par_errors_are_clear():
             ForceField.from_attract_par(text)
     with pytest.raises(ValueError, match="outside"):
         ForceField.from_attract_par(good, rec_types=[1, 3])
+
+
+def test_invalid_geometry_is_rejected_by_both_count_entry_points():
+    """att_nbgrid_count and att_nbgrid_count_noalloc take the same arguments
+    and apply the same geometry rules (validation answers before any CUDA
+    call, so this runs without a GPU)."""
+    from attract_b200 import _lib
+
+    lib = _lib.load(_lib_path())
+    bad = []
+    for field, value in (("dim", [1, 4, 4]), ("dim2", [-1, 2, 2]), ("spacing", 0.0), ("plateau", -1.0),
+                         ("n_types", 0)):
+        g = _lib.AttGridGeom()
+        g.dim[:] = [4, 4, 4]
+        g.dim2[:] = [2, 2, 2]
+        g.spacing, g.plateau, g.n_types = 1.0, 3.0, 1
+        if isinstance(value, list):
+            getattr(g, field)[:] = value
+        else:
+            setattr(g, field, value)
+        bad.append(g)
+    for g in bad:
+        rc0 = lib.att_nbgrid_count(C.byref(g), None, 0, 1.0, None, None, None, 0, None)
+        msg0 = lib.att_last_error_string()
+        rc1 = lib.att_nbgrid_count_noalloc(C.byref(g), None, 0, 1.0, None, None, None)
+        msg1 = lib.att_last_error_string()
+        assert rc0 == rc1 == 1, (rc0, rc1)
+        assert msg0 == msg1, (msg0, msg1)
+
+
+def test_list_total_beyond_32_bit_starts_is_rejected():
+    """The CSR starts are 32-bit: a neighbour grid whose entry total does not
+    fit is refused before the lists are allocated or filled."""
+    from attract_b200 import grid
+
+    grid.check_list_total(0)
+    grid.check_list_total(2 ** 32 - 1)
+    with pytest.raises(ValueError, match="32-bit"):
+        grid.check_list_total(2 ** 32)

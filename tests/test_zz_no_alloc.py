@@ -85,3 +85,17 @@ def test_noalloc_rejects_grids_beyond_the_fixed_workspace():
                                       torch.cuda.current_stream().cuda_stream)
     assert rc == 1
     assert b"fixed workspace" in lib.att_last_error_string()
+
+
+def test_noalloc_count_at_exactly_the_maximum_grid():
+    """A grid of exactly ATT_NBGRID_NOALLOC_MAX_VOXELS points (256 x 256 x 128),
+    where the count kernel writes the last word of the fixed array, equals the
+    entry point with a caller workspace."""
+    L, lib = _lib()
+    rec, n_rec = _receptor(400, 4)
+    gc = _geom((256, 256, 128), (-60.0, -60.0, -30.0), spacing=0.47)
+    assert gc.dim[0] * gc.dim[1] * gc.dim[2] == 8192 * 1024
+    h1, t1 = _count(L, lib, gc, rec, n_rec, 5.0, noalloc=True)
+    h0, t0 = _count(L, lib, gc, rec, n_rec, 5.0, noalloc=False)
+    assert t1 == t0 and t0 > 0
+    assert np.array_equal(h1, h0)

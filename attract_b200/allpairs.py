@@ -30,7 +30,10 @@ class AllPairs:
         if len(lig_type) == 0 or lig_type.min() < 0 or lig_type.max() >= ff.n_ltypes:
             raise ValueError("ligand type outside the force field (or no ligand beads)")
         self.n_rec = len(rec_type)
-        self.rec = pack_receptor(rec_xyz, rec_type, self.device)
+        # receptor beads grouped by type: the kernel reloads a pair-table row
+        # only when the receptor type changes (the sum does not depend on the order)
+        order = np.argsort(rec_type, kind="stable")
+        self.rec = pack_receptor(np.asarray(rec_xyz, np.float64).reshape(-1, 3)[order], rec_type[order], self.device)
         self.lig = pack_receptor(lig_xyz, lig_type, self.device)
         self.n_lig = len(lig_type)
         self.ff = ff

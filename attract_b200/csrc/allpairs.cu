@@ -3,14 +3,17 @@
 // test-energy.py:46-58 (delta over all pairs, nonbon of every d^2, summed per
 // structure), with ATTRACT's --rcut as an optional distance cutoff.
 //
-// One block per pose (grid-stride over poses).  The receptor streams through
-// shared memory in tiles of ALLPAIRS_TILE beads.  A thread holds one ligand
-// bead in registers and takes a slice of every tile: with n ligand beads,
-// 256 / n threads share each bead (a small ligand still fills the block), so
-// a warp reads at most a few receptor beads at a time (broadcasts).  Per-thread
-// sums (energy in float, force, lever-arm products) are reduced over the block
-// in double; the torque is linear in the force, so partial forces of one bead
-// add up correctly.
+// One block of 8 warps per pose (grid-stride over poses).  The receptor streams
+// through shared memory in tiles of AP_TILE beads; a warp takes one ligand bead
+// at a time against 32 consecutive receptor beads per step (conflict-free
+// 16-byte shared loads).  The pair-parameter row depends on the receptor type:
+// a lane keeps the last row it loaded and reloads only when the type changes,
+// so a receptor sorted by type (the host wrapper sorts it) reads each row once
+// per run of equal types instead of once per pair.  Per bead, the warp's lane
+// sums (energy and force, float) are reduced with shuffles and added to the
+// bead's accumulator in shared memory (double); the torque -- or x (x) g for the
+// 4x4 form -- is formed once per bead from its total force, and the block sums
+// the beads in double.
 #include <math.h>
 
 #include "common.cuh"
@@ -18,8 +21,12 @@
 namespace att {
 int report_error(int code, const char* msg);
 
-constexpr int ALLPAIRS_THREADS = 256;
-constexpr int ALLPAIRS_TILE = 1024;  // receptor beads per shared-memory tile (16 KB)
+constexpr int AP_THREADS = 256;
+constexpr int AP_WARPS = AP_THREADS / 32;
+constexpr int AP_TILE = 2048;   // receptor beads per shared-memory tile (32 KB)
+constexpr int AP_BEADS = 512;   // ligand beads per pass (their accumulators: 16 KB)
+constexpr size_t AP_SMEM = (size_t)AP_TILE * sizeof(float4) + (size_t)AP_BEADS * 4 * sizeof(double) +
+                           (size_t)AP_WARPS * 13 * sizeof(double);
 
 struct AllPairsParams {
   const float4* rec;   // [n_rec] x, y, z, receptor type (int bits)
@@ -48,16 +55,26 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
       double s = 0.0;
-      for (int w = 0; w < ALLPAIRS_THREADS / 32; ++w) s += red[w * NV + k];
+      for (int w = 0; w < AP_WARPS; ++w) s += red[w * NV + k];
       v[k] = s;
     }
   }
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(ALLPAIRS_THREADS) allpairs_kernel(const __grid_constant__ AllPairsParams p) {
-  __shared__ float4 s_rec[ALLPAIRS_TILE];
-  __shared__ double red[(ALLPAIRS_THREADS / 32) * 13];
+// 1/d2: the approximate reciprocal refined by one Newton step (within 1 ulp)
+__device__ __forceinline__ float recip_nr(float d2) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d2));
+  return r * fmaf(-d2, r, 2.f);
+}
+
+__global__ void __launch_bounds__(AP_THREADS) allpairs_kernel(const __grid_constant__ AllPairsParams p) {
+  extern __shared__ __align__(16) unsigned char ap_smem[];
+  float4* s_rec = reinterpret_cast<float4*>(ap_smem);
+  double* s_acc = reinterpret_cast<double*>(ap_smem + (size_t)AP_TILE * sizeof(float4));  // [AP_BEADS][4]
+  double* red = s_acc + AP_BEADS * 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool mat = p.pose_format == 1;
   for (int b = blockIdx.x; b < p.n_poses; b += gridDim.x) {
     // pose -> row-vector rotation M (X = x M + t) and, for Euler poses, the angles
@@ -86,72 +103,97 @@ __global__ void __launch_bounds__(ALLPAIRS_THREADS) allpairs_kernel(const __grid
 #pragma unroll
       for (int c = 0; c < 3; ++c) t[c] = __ldg(P + 3 + c);
     }
-    // per thread: energy, force, and the lever-arm sums (torque, or x (x) g for the 4x4 form)
+    // energy, force and the lever-arm sums (torque, or x (x) g for the 4x4 form)
     double acc[13];
 #pragma unroll
     for (int k = 0; k < 13; ++k) acc[k] = 0.0;
-    // threads per bead (receptor slices) and this thread's bead / slice
-    const int nsl = p.n_lig < ALLPAIRS_THREADS ? ALLPAIRS_THREADS / p.n_lig : 1;
-    const int per = ALLPAIRS_THREADS / nsl;  // beads per pass
-    const int sl = (int)threadIdx.x / per;
-    for (int i0 = 0; i0 < p.n_lig; i0 += per) {
-      const int i = i0 + (int)threadIdx.x % per;
-      const bool live = i < p.n_lig && sl < nsl;
-      float4 x = live ? __ldg(p.lig + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-      const int lt = live ? __float_as_int(x.w) : -1;
-      const float X = fmaf(x.x, m[0], fmaf(x.y, m[3], fmaf(x.z, m[6], t[0])));
-      const float Y = fmaf(x.x, m[1], fmaf(x.y, m[4], fmaf(x.z, m[7], t[1])));
-      const float Z = fmaf(x.x, m[2], fmaf(x.y, m[5], fmaf(x.z, m[8], t[2])));
-      const bool lok = live && (unsigned)lt < (unsigned)p.n_ltypes;
-      const float4* prow = p.pair + (long long)(lok ? lt : 0) * p.n_rtypes * 2;
-      float e = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-      for (int j0 = 0; j0 < p.n_rec; j0 += ALLPAIRS_TILE) {
-        const int nt = min(ALLPAIRS_TILE, p.n_rec - j0);
+    for (int i0 = 0; i0 < p.n_lig; i0 += AP_BEADS) {
+      const int nb = min(AP_BEADS, p.n_lig - i0);
+      for (int k = threadIdx.x; k < nb * 4; k += AP_THREADS) s_acc[k] = 0.0;
+      for (int j0 = 0; j0 < p.n_rec; j0 += AP_TILE) {
+        const int nt = min(AP_TILE, p.n_rec - j0);
         __syncthreads();  // the previous tile has been read
-        for (int j = threadIdx.x; j < nt; j += ALLPAIRS_THREADS) s_rec[j] = __ldg(p.rec + j0 + j);
+        for (int j = threadIdx.x; j < nt; j += AP_THREADS) s_rec[j] = __ldg(p.rec + j0 + j);
         __syncthreads();
-        if (lok) {
-          for (int j = sl; j < nt; j += nsl) {
+        for (int i = i0 + warp; i < i0 + nb; i += AP_WARPS) {  // warp-uniform
+          const float4 x = __ldg(p.lig + i);
+          const int lt = __float_as_int(x.w);
+          if ((unsigned)lt >= (unsigned)p.n_ltypes) continue;  // no pair table row: contributes nothing
+          const float X = fmaf(x.x, m[0], fmaf(x.y, m[3], fmaf(x.z, m[6], t[0])));
+          const float Y = fmaf(x.x, m[1], fmaf(x.y, m[4], fmaf(x.z, m[7], t[1])));
+          const float Z = fmaf(x.x, m[2], fmaf(x.y, m[5], fmaf(x.z, m[8], t[2])));
+          const float4* prow = p.pair + (size_t)lt * p.n_rtypes * 2;
+          float e = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+          int cur = -1;
+          float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;  // rc, ac, emin, rmin2 / ivor, eplat, -, rcap2
+          for (int j = lane; j < nt; j += 32) {
             const float4 r = s_rec[j];
             const int rt = __float_as_int(r.w);
             const float dx = X - r.x, dy = Y - r.y, dz = Z - r.z;
             const float dsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const bool hit = ((unsigned)rt < (unsigned)p.n_rtypes) & ((p.rcut2 <= 0.f) | (dsq < p.rcut2));
-            float4 p0, p1;  // rc, ac, emin, rmin2 / ivor, eplat, -, rcap2
-            ldg_f4x2(prow + (hit ? rt : 0) * 2, p0, p1);
+            const int rtc = hit ? rt : 0;
+            if (rtc != cur) {  // a new receptor type: its row
+              ldg_f4x2(prow + rtc * 2, p0, p1);
+              cur = rtc;
+            }
             const float d2 = fmaxf(dsq, p1.w);
-            const float rr2 = 1.0f / d2;
+            const float rr2 = recip_nr(d2);
             const float rr6 = rr2 * rr2 * rr2;
             const float vlj = fmaf(p0.x, rr2, -p0.y) * rr6;
             const bool near = d2 < p0.w;
             const float en = near ? fmaf(p1.x - 1.f, p0.z, vlj) : p1.x * vlj;
-            float gm = rr6 * rr2 * fmaf(-4.f * p0.x, rr2, 3.f * p0.y);
-            gm = near ? gm : p1.x * gm;
-            gm = (dsq < p1.w) ? 0.f : gm;
-            const float gf = hit ? 2.f * gm : 0.f;
+            float gm2 = rr6 * rr2 * fmaf(-8.f * p0.x, rr2, 6.f * p0.y);  // 2 dnonbon/d(d^2)
+            gm2 = near ? gm2 : p1.x * gm2;
+            gm2 = (dsq < p1.w) ? 0.f : gm2;
+            const float gf = hit ? gm2 : 0.f;
             e += hit ? en - p1.y : 0.f;
             gx = fmaf(gf, dx, gx);
             gy = fmaf(gf, dy, gy);
             gz = fmaf(gf, dz, gz);
           }
+#pragma unroll
+          for (int off = 16; off >= 1; off >>= 1) {
+            e += __shfl_xor_sync(0xffffffffu, e, off);
+            gx += __shfl_xor_sync(0xffffffffu, gx, off);
+            gy += __shfl_xor_sync(0xffffffffu, gy, off);
+            gz += __shfl_xor_sync(0xffffffffu, gz, off);
+          }
+          if (lane == 0) {  // bead i belongs to this warp alone
+            double* a = s_acc + (i - i0) * 4;
+            a[0] += e;
+            a[1] += gx;
+            a[2] += gy;
+            a[3] += gz;
+          }
         }
       }
-      acc[0] += e;
-      acc[1] += gx;
-      acc[2] += gy;
-      acc[3] += gz;
-      if (mat) {  // dE/dM[r][c] = sum_i x_r g_c
-        const float xr[3] = {x.x, x.y, x.z}, gc[3] = {gx, gy, gz};
+      __syncthreads();  // every warp's accumulators written (or just cleared)
+      // per bead of this pass: energy, force and its lever-arm terms
+      for (int i = i0 + threadIdx.x; i < i0 + nb; i += AP_THREADS) {
+        const double* a = s_acc + (i - i0) * 4;
+        const double e = a[0], gx = a[1], gy = a[2], gz = a[3];
+        const float4 x = __ldg(p.lig + i);
+        acc[0] += e;
+        acc[1] += gx;
+        acc[2] += gy;
+        acc[3] += gz;
+        if (mat) {  // dE/dM[r][c] = sum_i x_r g_c
+          const double xr[3] = {x.x, x.y, x.z}, gc[3] = {gx, gy, gz};
 #pragma unroll
-        for (int r = 0; r < 3; ++r)
+          for (int r = 0; r < 3; ++r)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) acc[4 + r * 3 + c] += (double)xr[r] * gc[c];
-      } else {  // torque about the pose centre: (X - t) x g
-        const float ax = X - t[0], ay = Y - t[1], az = Z - t[2];
-        acc[4] += (double)ay * gz - (double)az * gy;
-        acc[5] += (double)az * gx - (double)ax * gz;
-        acc[6] += (double)ax * gy - (double)ay * gx;
+            for (int c = 0; c < 3; ++c) acc[4 + r * 3 + c] += xr[r] * gc[c];
+        } else {  // torque about the pose centre: (X - t) x g, X - t = x M
+          const double ax = fmaf(x.x, m[0], fmaf(x.y, m[3], x.z * m[6]));
+          const double ay = fmaf(x.x, m[1], fmaf(x.y, m[4], x.z * m[7]));
+          const double az = fmaf(x.x, m[2], fmaf(x.y, m[5], x.z * m[8]));
+          acc[4] += ay * gz - az * gy;
+          acc[5] += az * gx - ax * gz;
+          acc[6] += ax * gy - ay * gx;
+        }
       }
+      __syncthreads();  // the accumulators are read before the next pass clears them
     }
     block_sum<13>(acc, red);
     if (threadIdx.x == 0) {
@@ -217,9 +259,14 @@ extern "C" int att_allpairs_energy(const float* rec_dev, int n_rec, const float*
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int blocks = (int)min((long long)n_poses, (long long)sms * 8);
-  allpairs_kernel<<<blocks, ALLPAIRS_THREADS, 0, (cudaStream_t)stream>>>(p);
-  const cudaError_t e = cudaGetLastError();
+  cudaError_t e = cudaFuncSetAttribute(allpairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AP_SMEM);
+  if (e != cudaSuccess) return report_error(ATT_E_CUDA, cudaGetErrorString(e));
+  int per_sm = 1;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, allpairs_kernel, AP_THREADS, AP_SMEM);
+  if (e != cudaSuccess) return report_error(ATT_E_CUDA, cudaGetErrorString(e));
+  const int blocks = (int)min((long long)n_poses, (long long)sms * max(per_sm, 1));
+  allpairs_kernel<<<blocks, AP_THREADS, AP_SMEM, (cudaStream_t)stream>>>(p);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return report_error(ATT_E_CUDA, cudaGetErrorString(e));
   return ATT_OK;
 }

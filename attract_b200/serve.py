@@ -16,6 +16,13 @@ not depend on what it was batched with: per-pose arithmetic is independent
 of the other poses of a launch, and the launch shape depends on the request
 alone.
 
+Rounds are pipelined: a round is enqueued while the previous one still runs
+(at most ``max_rounds_in_flight``), so the GPU does not wait for the host's
+admission and retirement work between rounds.  A request's last round copies
+its results into a pinned host mirror of the pose pool on the same stream, and
+the request is retired when that round's completion event has fired; its
+pool rows are reused only by work enqueued after those copies.
+
 Latency is wall-clock from ``submit`` to completion; ``stats()`` reports
 p50/p99 latency and sustained poses/s.  Every finished request can be logged
 as one JSON line (``log_path``), and :meth:`DockingServer.snapshot` /
@@ -149,12 +156,13 @@ class DockingServer:
     def __init__(self, grids, steps: int = 200, round_steps: int = 25, max_inflight_poses: int = 1_000_000,
                  hbm_budget_bytes: float = 150e9, adam: AdamOptions | None = None, opts: EvalOptions | None = None,
                  launch: LaunchShape | None = None, device=None, log_path: str | None = None,
-                 lanes_for=None, concurrent: bool = True):
+                 lanes_for=None, concurrent: bool = True, max_rounds_in_flight: int = 2):
         """``launch``: block size / block count of every launch;
         ``lanes_for``: ligand bead count -> lanes per pose (8, 16 or 32),
         by default :func:`lanes_by_size`; ``concurrent``: the shape groups of
         a round run on their own streams (else one after another on the
-        current stream)."""
+        current stream); ``max_rounds_in_flight``: rounds enqueued on the GPU
+        before the host waits for the oldest (1 = a synchronous loop)."""
         if steps % round_steps:
             raise ValueError("steps must be a multiple of round_steps")
         if len(grids) > 8:
@@ -179,6 +187,12 @@ class DockingServer:
         self.pose = torch.zeros((cap, 6), dtype=torch.float32, device=d)
         self.state = torch.zeros((cap, 12), dtype=torch.float32, device=d)
         self.scratch = MinimiseScratch(cap, d)
+        # pinned host mirror of the pool's results (pose, energy, status), same rows
+        self.h_pose = torch.empty((cap, 6), dtype=torch.float32).pin_memory()
+        self.h_energy = torch.empty(cap, dtype=torch.float32).pin_memory()
+        self.h_status = torch.empty(cap, dtype=torch.int32).pin_memory()
+        self.max_rounds_in_flight = max(1, int(max_rounds_in_flight))
+        self._inflight: deque = deque()  # (start event, end event, finishing requests, tables) per round
         self.pending: deque[Request] = deque()
         self.active: list[Request] = []
         self.done: list[Request] = []
@@ -203,11 +217,22 @@ class DockingServer:
         return req
 
     def idle(self) -> bool:
-        return not self.pending and not self.active
+        return not self.pending and not self.active and not self._inflight
 
     def run_until_idle(self):
         while not self.idle():
             self.round()
+        self.drain()
+
+    def drain(self):
+        """Wait for every enqueued round and retire its finished requests."""
+        while self._inflight:
+            self._retire_oldest()
+
+    def poll(self):
+        """Retire the rounds that have completed, without waiting."""
+        while self._inflight and self._inflight[0][1].query():
+            self._retire_oldest()
 
     def stats(self, since: float | None = None) -> dict:
         reqs = [r for r in self.done if since is None or r.arrival >= since]
@@ -258,12 +283,16 @@ class DockingServer:
         return g
 
     def round(self, now: float | None = None):
-        """Admit what fits, advance every active request by round_steps, retire finished ones."""
+        """Retire completed rounds, admit what fits, and enqueue one round that
+        advances every active request by round_steps ADAM steps."""
+        self.poll()
         now = time.perf_counter() if now is None else now
         torch.cuda.nvtx.range_push("serve.admit")
         self._admit(now)
         torch.cuda.nvtx.range_pop()
         if not self.active:
+            if self._inflight:
+                self._retire_oldest()
             return
         torch.cuda.nvtx.range_push("serve.round")
         groups = {}
@@ -272,18 +301,17 @@ class DockingServer:
         main = torch.cuda.current_stream(self.device)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(main)
-        # The groups' segment tables are allocated on the current stream and
-        # read by kernels on the groups' streams: they stay referenced until
-        # the round has synchronised, so the caching allocator cannot hand
-        # their memory to another group's tables while a kernel reads them.
+        # every group's tables first (uploaded on the current stream), then the
+        # launches, each group on its own stream, so that the groups overlap;
+        # the tables stay referenced until the round is retired
         tables = []
-        # the largest beads-per-lane groups first: their tiles take longest
-        for shape in sorted(groups, key=lambda sh: (-sh[1], -sh[0])):
+        for shape in sorted(groups, key=lambda sh: (-sh[1], -sh[0])):  # longest tiles first
             reqs = sorted(groups[shape], key=launch_order)
             lig_key, ligs, counter, stream = self._group(shape, reqs)
             segs = [Segment(r.receptor, i, r.n, r.step, r.slot0) for i, r in enumerate(reqs)]
             wl = Workload(self.grids, ligs, segs, shape[0], self.device, n_poses=self.capacity)
-            tables.append(wl)
+            tables.append((shape, wl, ligs, counter, stream))
+        for shape, wl, ligs, counter, stream in tables:
             scratch = _GroupScratch(self.scratch, counter)
             launch = LaunchShape(shape[0], self.launch.block_threads, self.launch.blocks, self.launch.test_flags)
             if stream is not None:
@@ -291,32 +319,60 @@ class DockingServer:
             with torch.cuda.stream(stream if stream is not None else main):
                 minimise(wl, self.pose, self.round_steps, self.adam, self.opts, pose_out=self.pose,
                          adam_state=self.state, launch=launch, scratch=scratch)
+            self.launches += 1
+        for shape, wl, ligs, counter, stream in tables:
             if stream is not None:
                 main.wait_stream(stream)
-            self.launches += 1
-        e1.record(main)
-        e1.synchronize()
-        del tables
-        self.gpu_ms += e0.elapsed_time(e1)
-        self.rounds += 1
-        torch.cuda.nvtx.range_pop()
-        torch.cuda.nvtx.range_push("serve.retire")
-        t = time.perf_counter()
-        still = []
+        # requests that finish with this round: results to the pinned mirror,
+        # ordered after the round on the current stream; their rows go back to
+        # the pool (later writes to them are enqueued after these copies)
+        still, finishing = [], []
         for r in self.active:
             r.step += self.round_steps
-            if r.step >= self.steps:
+            (finishing if r.step >= self.steps else still).append(r)
+        if finishing:
+            rows = [(r.slot0, r.n) for r in finishing]
+            # a mirror row that still holds an unretired request's results is
+            # retired first (only when a request finishes in its first round)
+            while self._inflight and any(_overlap(rows, (q.slot0, q.n)) for q in self._unretired()):
+                self._retire_oldest()
+            for r in finishing:
                 sl = slice(r.slot0, r.slot0 + r.n)
-                r.result_poses = self.pose[sl].cpu().numpy()
-                r.result_energies = self.scratch.energy[sl].cpu().numpy()
-                r.result_status = self.scratch.status[sl].cpu().numpy()
-                r.finished = t
+                self.h_pose[sl].copy_(self.pose[sl], non_blocking=True)
+                self.h_energy[sl].copy_(self.scratch.energy[sl], non_blocking=True)
+                self.h_status[sl].copy_(self.scratch.status[sl], non_blocking=True)
                 self.pool.release(r.slot0, r.n)
-                self.done.append(r)
-                self._log(r)
-            else:
-                still.append(r)
+        e1.record(main)
+        self._inflight.append((e0, e1, finishing, tables))
         self.active = still
+        self.rounds += 1
+        torch.cuda.nvtx.range_pop()
+        # with k = max_rounds_in_flight, wait until at most k - 1 rounds are
+        # outstanding: k = 2 keeps this round queued while the host prepares
+        # the next one; k = 1 is a synchronous loop
+        while len(self._inflight) >= self.max_rounds_in_flight:
+            self._retire_oldest()
+
+    def _unretired(self):
+        for _, _, fin, _ in self._inflight:
+            yield from fin
+
+    def _retire_oldest(self):
+        """Wait for the oldest enqueued round; retire the requests it finished."""
+        torch.cuda.nvtx.range_push("serve.retire")
+        e0, e1, finishing, tables = self._inflight.popleft()
+        e1.synchronize()
+        self.gpu_ms += e0.elapsed_time(e1)
+        t = time.perf_counter()
+        for r in finishing:
+            sl = slice(r.slot0, r.slot0 + r.n)
+            r.result_poses = self.h_pose[sl].numpy().copy()
+            r.result_energies = self.h_energy[sl].numpy().copy()
+            r.result_status = self.h_status[sl].numpy().copy()
+            r.finished = t
+            self.done.append(r)
+            self._log(r)
+        del tables
         torch.cuda.nvtx.range_pop()
 
     def _log(self, r: Request):
@@ -338,6 +394,7 @@ class DockingServer:
         """The unfinished requests, between rounds: per active request its
         current poses, ADAM moments and step; pending requests as submitted.
         Plain NumPy / Python values (``numpy.savez`` / pickle friendly)."""
+        self.drain()
         torch.cuda.synchronize(self.device)
         reqs = []
         for r in self.active:
@@ -359,6 +416,11 @@ class DockingServer:
             req = Request(q["receptor"], q["ligand"], q["poses"], adam0=q["adam"], step0=int(q["step"]))
             srv.submit(req, now=q["arrival"])
         return srv
+
+
+def _overlap(rows, span) -> bool:
+    s, n = span
+    return any(a < s + n and s < a + m for a, m in rows)
 
 
 def replay(server: DockingServer, requests, duration: float | None = None, time_scale: float = 1.0,
@@ -386,6 +448,7 @@ def replay(server: DockingServer, requests, duration: float | None = None, time_
             time.sleep(min(0.001, max(0.0, queue[0]["t"] * time_scale - now)))
             continue
         server.round()
+    server.drain()
     st = server.stats(since=t0)
     st["arrived"] = arrived
     st["window_s"] = time.perf_counter() - t0

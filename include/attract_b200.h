@@ -318,8 +318,10 @@ int att_nbgrid_count_noalloc(const AttGridGeom* geom, const float* rec_dev, int 
    receptor type (int32 bits); lig_dev [n_lig][4] x, y, z, ligand type (int32
    bits); pose_dev [B][6] (pose_format 0) or [B][16] row-vector 4x4 (1);
    energy_dev [B]; grad_dev [B][6] dE/d(Euler, t) or [B][16] dE/dmat, may be
-   NULL.  Replaces main() of test-energy.py:46-58 (the reference's rescoring;
-   ATTRACT --score with --rcut). */
+   NULL.  Receptor beads grouped by type run faster (a pair-parameter row is
+   reloaded only where the receptor type changes); the result does not depend
+   on their order beyond float32 summation order.  Replaces main() of
+   test-energy.py:46-58 (the reference's rescoring; ATTRACT --score with --rcut). */
 int att_allpairs_energy(const float* rec_dev, int n_rec, const float* lig_dev, int n_lig,
                         const float* pose_dev, int n_poses, int pose_format, const float* pair_dev,
                         int n_rtypes, int n_ltypes, float rcut, float* energy_dev, float* grad_dev,

@@ -19,7 +19,11 @@ counted float32 bound (``float32_bounds``):
   the translation and the grid-frame shift): the spread of each bead's
   float64 energy and gradient over +-2 delta along each axis, which covers
   the slope and any jump within reach (a cell face of the analytic gradient,
-  the energy cap, the inner/outer grid boundary).
+  the energy cap, the inner/outer grid boundary);
+* the trilinear quirk: the reference's floor/ceil weights give 0 for a bead
+  whose voxel coordinate is an exact integer; a float32 coordinate within
+  reach of an integer (about one bead in 30 000) may land on it and lose
+  its whole grid term, which the float64 coordinate does not.
 """
 from __future__ import annotations
 
@@ -150,6 +154,20 @@ def float32_bounds(poses, lig, gt, lt, G, mode):
         Em, gm = O.bead_energrad(X - d, gt, lt, G, mode)
         sE = np.maximum(sE, np.abs(Ep - Em))
         sG = np.maximum(sG, np.linalg.norm(gp - gm, axis=-1))
+    # the reference's floor/ceil weights zero a bead whose voxel coordinate is
+    # an exact integer (test5.py:256-259): a float32 coordinate within reach
+    # of an integer may land on it, which removes the bead's whole grid term
+    g = G["geom"]
+    v = (X - o) / g["spacing"]
+    inn = np.all((v >= 0) & (v < np.asarray(g["dim"]) - 1), axis=-1)
+    vo = (v + g["extension"]) / 2.0
+    vv = np.where(inn[..., None], v, vo)
+    dv = np.where(inn, 1.0, 0.5)[..., None] * (2 * delta[..., None] / g["spacing"] + 8 * U * np.abs(vv))
+    on_int = np.any(np.abs(vv - np.round(vv)) <= dv, axis=-1)
+    qE = np.where(on_int, Eg, 0.0)
+    qG = np.where(on_int, np.linalg.norm(np.abs(gg), axis=-1), 0.0)
+    sE = sE + qE
+    sG = sG + qG
     arm = 1.0 + np.linalg.norm(X - t, axis=-1)
     gnorm = np.linalg.norm(gb, axis=-1)
     bE = 32 * U * S_e.sum(1) + sE.sum(1)

@@ -231,7 +231,7 @@ def test_config3_finite_differences_poses_and_voxels():
     vox = touched[rng.choice(len(touched), 256, replace=False)]
     inner64 = G["inner"].astype(np.float64)
     G64 = dict(G, inner=inner64)
-    worst = 0.0
+    worst = worst_bound = 0.0
     for t_, x_, y_, z_ in vox:
         near = inn & (gt[None, :] == t_) & np.all(
             (base >= np.array([x_, y_, z_]) - 1) & (base <= np.array([x_, y_, z_])), axis=2)
@@ -244,8 +244,12 @@ def test_config3_finite_differences_poses_and_voxels():
         Em = O.energrad(poses[rows], lig, gt, lt, G64, mode="analytic")[0].sum()
         inner64[t_, x_, y_, z_, 0] = old
         fdv = (Ep - Em) / (2 * h)
+        # the kernel adds the voxel's weights one by one in float32 (atomics):
+        # n positive terms carry at most n u of relative error
+        n_terms = int(near.sum())
         err = abs(din[t_, x_, y_, z_, 0] - fdv) / max(1.0, abs(fdv))
         worst = max(worst, err)
-    print(f"\n[fd voxels] 256 voxels, max relative error {worst:.2e}")
-    # float32 atomic accumulation of up to a few hundred weights per voxel
-    assert worst <= 1e-5, worst
+        worst_bound = max(worst_bound, err / max(1e-5, 2 * n_terms * 2.0 ** -24))
+    print(f"\n[fd voxels] 256 voxels, max relative error {worst:.2e} "
+          f"({worst_bound:.2f} of max(1e-5, float32 accumulation bound))")
+    assert worst_bound <= 1.0, (worst, worst_bound)

@@ -250,7 +250,9 @@ cudaError_t launch_nb_fill(const AttGridGeom& g, const float* rec, int n_rec, fl
   return cudaGetLastError();
 }
 
-// CSR -> fixed-size records {u32 overflow index, u16 count, inline entries}
+// CSR -> fixed-size records {inline entries, u16 count, u32 overflow index}:
+// the entries start the record, so that a reader takes four at a time in
+// 8-byte loads
 __global__ void nb_pack_kernel(const uint2* __restrict__ hdr, const uint16_t* __restrict__ list, long long nvox,
                                int rec_bytes, unsigned char* __restrict__ out) {
   const int inl = ATT_NB_INLINE(rec_bytes);
@@ -258,10 +260,10 @@ __global__ void nb_pack_kernel(const uint2* __restrict__ hdr, const uint16_t* __
        v += (long long)gridDim.x * blockDim.x) {
     const uint2 h = hdr[v];
     unsigned char* r = out + v * rec_bytes;
-    *reinterpret_cast<unsigned*>(r) = h.x + (unsigned)inl;
-    uint16_t* e = reinterpret_cast<uint16_t*>(r + 4);
-    e[0] = (uint16_t)min(h.y, 65535u);
-    for (int i = 0; i < inl; ++i) e[1 + i] = (i < (int)h.y) ? list[h.x + i] : (uint16_t)ATT_NB_EMPTY;
+    uint16_t* e = reinterpret_cast<uint16_t*>(r);
+    for (int i = 0; i < inl; ++i) e[i] = (i < (int)h.y) ? list[h.x + i] : (uint16_t)ATT_NB_EMPTY;
+    *reinterpret_cast<uint16_t*>(r + rec_bytes - 6) = (uint16_t)min(h.y, 65535u);
+    *reinterpret_cast<unsigned*>(r + rec_bytes - 4) = h.x + (unsigned)inl;
   }
 }
 

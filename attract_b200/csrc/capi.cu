@@ -128,6 +128,7 @@ static int make_kgrid(const AttGrid* a, int gi, KGrid* k) {
   k->ext = (float)g.extension;
   k->plateau = g.plateau;
   k->plateau2 = g.plateau * g.plateau;
+  k->plateau_x2 = 2.f * g.plateau;
   k->dx = g.dim[0];
   k->dy = g.dim[1];
   k->dz = g.dim[2];

@@ -14,7 +14,7 @@ struct __align__(16) KGrid {
   float fdx1, fdy1, fdz1;         // inner dim - 1 (float, for the range test)
   float fex1, fey1, fez1;         // outer dim2 - 1
   float ext;                      // gridextension
-  float plateau, plateau2;
+  float plateau, plateau2, plateau_x2;  // plateau, its square, twice it
   int dx, dy, dz;                 // inner points
   int dx2, dy2, dz2;              // outer points
   int n_types;

@@ -36,6 +36,8 @@
 //   total, gravity       E_grid + E_nb + 0.1|t|^2       test5.py:404-420
 #include <math.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace att {
@@ -106,6 +108,18 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 __device__ __forceinline__ unsigned lds_u16(const void* p) {
   unsigned short v;
   asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(smem_u32(p)) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned lds_u32(const void* p) {
+  unsigned v;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ uint2 lds_u64(const void* p) {  // p 8-byte aligned
+  uint2 v;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(smem_u32(p)) : "memory");
   return v;
 }
 
@@ -183,29 +197,35 @@ __device__ __forceinline__ int find_segment(const KParams& p, int tile) {
 // Pair term of one (bead, receptor bead) list entry, branch-free: adds the
 // energy to e and returns dE/dx; a pair that is out of range (beyond the
 // plateau, bad type) adds 0 energy and returns a zero gradient.
+// The bead's ligand type is valid here: phase A gives a bead list entries only
+// when its type is inside the pair table.  NE: accumulate the energy too (the
+// minimiser's steps before the last need only the gradient).
+template <bool NE>
 __device__ __forceinline__ void pair_term_masked(const KParams& p, const KGrid& G, const BeadPos& bp,
                                                  const float4& r, float& e, float& gx, float& gy, float& gz) {
   const float dx = bp.x - r.x, dy = bp.y - r.y, dz = bp.z - r.z;
   const float dsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   const int rt = __float_as_int(r.w);
-  const bool hit =
-      (dsq < G.plateau2) & ((unsigned)rt < (unsigned)G.n_rtypes) & ((unsigned)bp.lt < (unsigned)G.n_ltypes);
+  const bool hit = (dsq < G.plateau2) & ((unsigned)rt < (unsigned)G.n_rtypes);
   const int idx = hit ? bp.lt * G.n_rtypes + rt : 0;
   float4 p0, p1;  // rc, ac, emin, rmin2 / ivor, eplat, gplat, rcap2: one 32-B row
-  ldg_f4x2(G.pair + (long long)idx * 2, p0, p1);
+  ldg_f4x2(G.pair + (size_t)(unsigned)idx * 2, p0, p1);
   const float d2 = fmaxf(dsq, p1.w);
   float rr2;  // approximate reciprocal (1 ulp): the pair energy carries ~4 ulp
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rr2) : "f"(d2));
   const float rr6 = rr2 * rr2 * rr2;
-  const float vlj = fmaf(p0.x, rr2, -p0.y) * rr6;
   const bool near = d2 < p0.w;
-  const float en = near ? fmaf(p1.x - 1.f, p0.z, vlj) : p1.x * vlj;
-  const float dv = rr6 * rr2 * fmaf(-4.f * p0.x, rr2, 3.f * p0.y);
-  float gm = near ? dv : p1.x * dv;
-  gm = (dsq < p1.w) ? 0.f : gm;
-  if (p.grad_mode == ATT_GRAD_REFERENCE) gm = fmaf(-p1.z * G.plateau, rsqrtf(dsq), gm);
-  const float gf = hit ? 2.f * gm : 0.f;
-  e += hit ? en - p1.y : 0.f;
+  if (NE) {
+    const float vlj = fmaf(p0.x, rr2, -p0.y) * rr6;
+    const float en = near ? fmaf(p1.x - 1.f, p0.z, vlj) : p1.x * vlj;
+    e += hit ? en - p1.y : 0.f;
+  }
+  // 2 dnonbon/d(d^2): the factor 2 of d(d^2)/dx folded into the constants
+  const float dv2 = rr6 * rr2 * fmaf(-8.f * p0.x, rr2, 6.f * p0.y);
+  float gm2 = near ? dv2 : p1.x * dv2;
+  gm2 = (dsq < p1.w) ? 0.f : gm2;
+  if (p.grad_mode == ATT_GRAD_REFERENCE) gm2 = fmaf(-p1.z * G.plateau_x2, rsqrtf(dsq), gm2);
+  const float gf = hit ? gm2 : 0.f;
   gx = gf * dx;
   gy = gf * dy;
   gz = gf * dz;
@@ -265,6 +285,10 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
 
   // statistics (MODE_MIN): bead evaluations with a brick, list lookups, list
   // entries, brick copies, record copies
+  // Only the 32-lane kernel with one bead per lane keeps them in registers;
+  // the other shapes add warp sums to the counters every step instead (in
+  // statistics launches only), which leaves their registers to the step.
+  constexpr bool STATS_REGS = (S == 32 && K == 1);
   unsigned c_grid = 0, c_look = 0, c_ent = 0, c_cpb = 0, c_cpr = 0;
   const bool want_stats = p.stats != nullptr;
 
@@ -465,6 +489,10 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         q22 = cpsi;
       }
 
+      // the energy is needed by every evaluation of the single-evaluation
+      // modes, and by the last evaluation of a minimisation (the one reported)
+      const bool need_e = (MODE != MODE_MIN && !QUAT) || (MODE == MODE_MIN && s == nsteps) ||
+                          (QUAT && s + 1 >= nsteps);
       float acc_e = 0.f, acc_gx = 0.f, acc_gy = 0.f, acc_gz = 0.f;
       float acc_t[ACC9 ? 9 : 3];
 #pragma unroll
@@ -478,8 +506,8 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
       float fx[K], fy[K], fz[K], gscale[K];
       int brick_gt[K], bix[K], biy[K], biz[K];  // grid slot, base voxel (for the adjoint scatter)
       bool use[K], outer_k[K];
-      long long bidx[K];  // brick index
-      long long nvox[K];  // nearest inner grid point for the list lookup, -1 = none
+      int bidx[K];  // brick index (< 2^31: checked on the host)
+      int nvox[K];  // nearest list-grid point for the list lookup, -1 = none (< 2^31: checked on the host)
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         const int i = tl + k * S;
@@ -498,7 +526,7 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         float ux = vx, uy = vy, uz = vz;
         float sc = G.inv_s;
         int ny = G.dy, nz = G.dz;
-        long long base = 0;
+        int base = 0;
         outer_k[k] = false;
         if (live && G.bricks != nullptr && gt < G.n_types) {
           u = inn;
@@ -510,7 +538,7 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
             sc = 0.5f * G.inv_s;
             ny = G.dy2;
             nz = G.dz2;
-            base = G.n_inner;
+            base = (int)G.n_inner;
             outer_k[k] = true;
           }
         }
@@ -526,15 +554,13 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         bix[k] = (int)flx;
         biy[k] = (int)fly;
         biz[k] = (int)flz;
-        bidx[k] = u ? (long long)gt * G.type_stride + base + ((long long)bix[k] * (ny - 1) + biy[k]) * (nz - 1) +
-                          biz[k]
-                    : 0;
+        bidx[k] = u ? gt * (int)G.type_stride + base + (bix[k] * (ny - 1) + biy[k]) * (nz - 1) + biz[k] : 0;
         nvox[k] = -1;
         if (inn && G.nb_rec != nullptr && lt < G.n_ltypes) {
           // nearest list-grid point (the inner grid point itself when nb_scale = 1)
           const int nx = (int)floorf(fmaf(vx, G.nb_scale, 0.5f)), my = (int)floorf(fmaf(vy, G.nb_scale, 0.5f)),
                     mz = (int)floorf(fmaf(vz, G.nb_scale, 0.5f));
-          nvox[k] = ((long long)nx * G.ndy + my) * G.ndz + mz;
+          nvox[k] = (nx * G.ndy + my) * G.ndz + mz;
         }
         if (use[k] && !ATT_CHECK(bidx[k] >= 0 && bidx[k] < G.n_bricks, 1, bidx[k], G.n_bricks)) use[k] = false;
         if (nvox[k] >= 0 && !ATT_CHECK(nvox[k] < G.n_vox, 2, nvox[k], G.n_vox)) nvox[k] = -1;
@@ -564,14 +590,30 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
       unsigned my_bytes = 0;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        need_b[k] = use[k] && (int)bidx[k] != held_b[k];
-        need_v[k] = nvox[k] >= 0 && (int)nvox[k] != held_v[k];
+        need_b[k] = use[k] && bidx[k] != held_b[k];
+        need_v[k] = nvox[k] >= 0 && nvox[k] != held_v[k];
         my_bytes += (need_b[k] ? 128u : 0u) + (need_v[k] ? (unsigned)G.nb_rec_bytes : 0u);
-        if (MODE == MODE_MIN && want_stats) {
+        if (MODE == MODE_MIN && STATS_REGS && want_stats) {
           c_grid += use[k] ? 1u : 0u;
           c_look += nvox[k] >= 0 ? 1u : 0u;
           c_cpb += need_b[k] ? 1u : 0u;
           c_cpr += need_v[k] ? 1u : 0u;
+        }
+      }
+      if (MODE == MODE_MIN && !STATS_REGS && want_stats) {
+        unsigned n4[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          n4[0] += use[k] ? 1u : 0u;
+          n4[1] += nvox[k] >= 0 ? 1u : 0u;
+          n4[2] += need_b[k] ? 1u : 0u;
+          n4[3] += need_v[k] ? 1u : 0u;
+        }
+        const int slot_of[4] = {0, 1, 3, 4};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const unsigned w = __reduce_add_sync(0xffffffffu, n4[i]);
+          if (lane == 0 && w) atomicAdd(p.stats + slot_of[i], (unsigned long long)w);
         }
       }
       const unsigned warp_bytes = __reduce_add_sync(0xffffffffu, my_bytes);
@@ -585,12 +627,13 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         for (int k = 0; k < K; ++k) {
           const int sk = tbase + tl + k * S;
           if (need_b[k]) {
-            bulk_copy(bricks + (size_t)sk * 8, G.bricks + bidx[k] * 8, 128u, bar);
-            held_b[k] = (int)bidx[k];
+            bulk_copy(bricks + (size_t)sk * 8, G.bricks + (size_t)bidx[k] * 8, 128u, bar);
+            held_b[k] = bidx[k];
           }
           if (need_v[k]) {
-            bulk_copy(nrec + (size_t)sk * RS, G.nb_rec + nvox[k] * G.nb_rec_bytes, (unsigned)G.nb_rec_bytes, bar);
-            held_v[k] = (int)nvox[k];
+            bulk_copy(nrec + (size_t)sk * RS, G.nb_rec + (size_t)nvox[k] * G.nb_rec_bytes, (unsigned)G.nb_rec_bytes,
+                      bar);
+            held_v[k] = nvox[k];
           }
         }
         bool done = mbar_try_wait(bar, parity);
@@ -617,15 +660,26 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
       // Teams with more pairs than the buffer holds take several windows.
       {
         const unsigned ninl = (unsigned)G.nb_inline;
+        const int RB = G.nb_rec_bytes;  // record: inline entries, u16 count at RB - 6, u32 overflow at RB - 4
         unsigned ck[K];
-        unsigned my_total = 0;
+        unsigned my_total = 0, my_in = 0;
+        bool my_ovf = false;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
           const unsigned char* rk = nrec + (size_t)(tbase + tl + k * S) * RS;
-          ck[k] = (nvox[k] >= 0) ? lds_u16(rk + 4) : 0u;
+          ck[k] = (nvox[k] >= 0) ? lds_u16(rk + RB - 6) : 0u;
           my_total += ck[k];
+          my_in = max(my_in, min(ck[k], ninl));
+          my_ovf |= ck[k] > ninl;
         }
-        if (MODE == MODE_MIN && want_stats) c_ent += my_total;
+        if (MODE == MODE_MIN && want_stats) {
+          if (STATS_REGS) {
+            c_ent += my_total;
+          } else {
+            const unsigned w = __reduce_add_sync(0xffffffffu, my_total);
+            if (lane == 0 && w) atomicAdd(p.stats + 2, (unsigned long long)w);
+          }
+        }
         unsigned incl = my_total;  // inclusive scan over the team's lanes
 #pragma unroll
         for (int off = 1; off < S; off <<= 1) {
@@ -635,33 +689,63 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         const unsigned team_total = __shfl_sync(0xffffffffu, incl, S - 1, S);
         const unsigned run0 = incl - my_total;  // buffer position of this lane's first entry
         const unsigned warp_max = __reduce_max_sync(0xffffffffu, team_total);
+        const unsigned warp_in = __reduce_max_sync(0xffffffffu, my_in);  // longest inline run of the warp
+        const bool any_ovf = __any_sync(0xffffffffu, my_ovf);
         for (unsigned q0 = 0; q0 < warp_max; q0 += PB) {
-          unsigned r = run0;
+          // inline entries, four per 8-byte shared load; a team whose pairs
+          // fit one window (the common case) needs no window test per entry
+          const bool one_window = warp_max <= (unsigned)PB;
+          for (unsigned c = 0; c < warp_in; c += 4) {
+            unsigned r = run0;
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const unsigned lo = max(q0, r), hi = min(r + ck[k], q0 + PB);
-            if (lo < hi) {
-              const unsigned char* rk = nrec + (size_t)(tbase + tl + k * S) * RS;
-              const unsigned ovf = *reinterpret_cast<const unsigned*>(rk);
-              const uint16_t* inl = reinterpret_cast<const uint16_t*>(rk + 6);
-              const unsigned tag = (unsigned)(tl + k * S) << 16;
-#ifdef ATT_BOUNDS_CHECK
-              if (ck[k] > ninl && !ATT_CHECK((long long)ovf - ninl + ck[k] <= G.n_list, 6, ovf, ck[k])) {
-                for (unsigned s = lo; s < hi; ++s) pb[s - q0] = ATT_NB_EMPTY | tag;
-                r += ck[k];
-                continue;
+            for (int k = 0; k < K; ++k) {
+              const unsigned nin = min(ck[k], ninl);
+              if (c < nin) {
+                const unsigned char* rk = nrec + (size_t)(tbase + tl + k * S) * RS;
+                const uint2 w = lds_u64(rk + 2 * c);
+                const unsigned tag = (unsigned)(tl + k * S) << 16;
+                const unsigned v4[4] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16};
+                if (one_window) {
+                  uint32_t* dst = pb + (r + c);
+#pragma unroll
+                  for (int i = 0; i < 4; ++i)
+                    if (c + i < nin) dst[i] = v4[i] | tag;
+                } else {
+#pragma unroll
+                  for (int i = 0; i < 4; ++i) {
+                    const unsigned pos = r + c + i - q0;
+                    if ((c + i < nin) & (pos < (unsigned)PB)) pb[pos] = v4[i] | tag;
+                  }
+                }
               }
-#endif
-              for (unsigned s = lo; s < hi; ++s) {
-                const unsigned e = s - r;
-                const unsigned j = (e < ninl) ? lds_u16(inl + e) : ldg_nc_u16(G.nb_list + (ovf + (e - ninl)));
-                pb[s - q0] = j | tag;
-              }
+              r += ck[k];
             }
-            r += ck[k];
+          }
+          if (any_ovf) {  // entries beyond the inline ones, from the CSR list
+            unsigned r = run0;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+              if (ck[k] > ninl) {
+                const unsigned char* rk = nrec + (size_t)(tbase + tl + k * S) * RS;
+                const unsigned ovf = lds_u32(rk + RB - 4);
+                const unsigned tag = (unsigned)(tl + k * S) << 16;
+                const unsigned lo = max(q0, r + ninl), hi = min(r + ck[k], q0 + PB);
+#ifdef ATT_BOUNDS_CHECK
+                if (!ATT_CHECK((long long)ovf - ninl + ck[k] <= G.n_list, 6, ovf, ck[k])) {
+                  for (unsigned s = lo; s < hi; ++s) pb[s - q0] = ATT_NB_EMPTY | tag;
+                  r += ck[k];
+                  continue;
+                }
+#endif
+                for (unsigned s = lo; s < hi; ++s) pb[s - q0] = ldg_nc_u16(G.nb_list + (ovf + (s - r - ninl))) | tag;
+              }
+              r += ck[k];
+            }
           }
           __syncwarp();
           const unsigned n = min(team_total - min(team_total, q0), (unsigned)PB);
+          auto pair_window = [&](auto ne) {
+          constexpr bool NE = decltype(ne)::value;
           for (unsigned s0 = tl; s0 < n; s0 += U * S) {
             unsigned ww[U];
 #pragma unroll
@@ -683,10 +767,13 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
               const unsigned bi = tbase + (ww[m] >> 16);
               const BeadPos bp = bpos[bi];
               float px, py, pz;
-              pair_term_masked(p, G, bp, rr[m], acc_e, px, py, pz);
-              BeadArm ba;  // lever arm: Q x = X - t (the 4x4 form needs the ligand-frame x)
+              pair_term_masked<NE>(p, G, bp, rr[m], acc_e, px, py, pz);
+              // moment arm: the bead position X (the torque about t, sum (X - t) x g,
+              // is sum X x g - t x sum g, formed after the team sum); the
+              // 4x4 form accumulates with the ligand-frame x
+              BeadArm ba;
               if (ACC9) ba = barm[bi];
-              else { ba.x = bp.x - tx; ba.y = bp.y - ty; ba.z = bp.z - tz; }
+              else { ba.x = bp.x; ba.y = bp.y; ba.z = bp.z; }
               acc_gx += px;
               acc_gy += py;
               acc_gz += pz;
@@ -701,11 +788,16 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
               }
             }
           }
+          };
+          if (need_e) pair_window(std::true_type{});
+          else pair_window(std::false_type{});
           __syncwarp();  // the next window overwrites the buffer
         }
       }
 
       // ---------------- phase D: grid term from the bricks in shared memory
+      auto phase_d = [&](auto ne) {
+      constexpr bool NE = decltype(ne)::value;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (use[k]) {
@@ -728,7 +820,7 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
             const float4 v = br[c];
             const float wx = (q & 4) ? wx1 : wx0, wy = (q & 2) ? wy1 : wy0, wz = (q & 1) ? wz1 : wz0;
             const float w = wx * wy * wz;
-            eb = fmaf(w, v.x, eb);
+            if (NE) eb = fmaf(w, v.x, eb);
             if (p.grad_mode == ATT_GRAD_REFERENCE) {
               gbx = fmaf(-w, v.y, gbx);
               gby = fmaf(-w, v.z, gby);
@@ -754,14 +846,14 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
               }
             }
           }
-          BeadArm ba;  // lever arm: Q x = X - t, as in the pair term (ACC9: ligand-frame x)
+          BeadArm ba;  // moment arm: the bead position X, as in the pair term (ACC9: ligand-frame x)
           if (ACC9) {
             ba = barm[tbase + tl + k * S];
           } else {
             const BeadPos bq = bpos[tbase + tl + k * S];
-            ba.x = bq.x - tx; ba.y = bq.y - ty; ba.z = bq.z - tz;
+            ba.x = bq.x; ba.y = bq.y; ba.z = bq.z;
           }
-          acc_e += eb;
+          if (NE) acc_e += eb;
           acc_gx += gbx;
           acc_gy += gby;
           acc_gz += gbz;
@@ -776,18 +868,26 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
           }
         }
       }
+      };
+      if (need_e) phase_d(std::true_type{});
+      else phase_d(std::false_type{});
       // the next chunk's / evaluation's bulk copies overwrite the slots read above
       __syncwarp();
       fence_proxy_async();
       }  // chunks
 
       // ---------------- team reduction and output / ADAM
-      acc_e = team_sum<S>(acc_e);
+      if (need_e) acc_e = team_sum<S>(acc_e);
       acc_gx = team_sum<S>(acc_gx);
       acc_gy = team_sum<S>(acc_gy);
       acc_gz = team_sum<S>(acc_gz);
 #pragma unroll
       for (int k = 0; k < (ACC9 ? 9 : 3); ++k) acc_t[k] = team_sum<S>(acc_t[k]);
+      if (!ACC9) {  // torque about the pose's translation: sum X x g - t x sum g
+        acc_t[0] -= fmaf(ty, acc_gz, -tz * acc_gy);
+        acc_t[1] -= fmaf(tz, acc_gx, -tx * acc_gz);
+        acc_t[2] -= fmaf(tx, acc_gy, -ty * acc_gx);
+      }
 
       if constexpr (QUAT) {
         // ---- SCHEMA protocol step (test5.py:450-458): energy and gradient
@@ -822,9 +922,11 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
           const float err = gk - my_m;  // against the previous first moment (optax scale_by_belief)
           my_m = fmaf(p.b1, my_m, (1.f - p.b1) * gk);
           my_v = fmaf(p.b2, my_v, (1.f - p.b2) * err * err) + p.eps_root;
-          const float mh = my_m / (float)(1.0 - bp1);
-          const float vh = my_v / (float)(1.0 - bp2);
-          my_x -= st_lr * mh / (sqrtf(vh) + p.eps);
+          // bias-corrected moments; approximate divisions (2 ulp) keep the
+          // update off the IEEE division's slow path
+          const float mh = __fdividef(my_m, (float)(1.0 - bp1));
+          const float vh = __fdividef(my_v, (float)(1.0 - bp2));
+          my_x -= __fdividef(st_lr * mh, sqrtf(vh) + p.eps);
         }
         normalise_quat();  // Rotation.from_quat(rotations.as_quat())
         if (k_stage >= st_epochs) {  // next stage: a fresh optimiser state
@@ -895,10 +997,12 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
       } else if (tl < 6) {
         my_m = fmaf(p.b1, my_m, (1.f - p.b1) * gk);
         my_v = fmaf(p.b2, my_v, (1.f - p.b2) * gk * gk);
-        const float mh = my_m / (float)(1.0 - bp1);
-        const float vh = my_v / (float)(1.0 - bp2);
+        // bias-corrected moments; approximate divisions (2 ulp) keep the
+        // update off the IEEE division's slow path
+        const float mh = __fdividef(my_m, (float)(1.0 - bp1));
+        const float vh = __fdividef(my_v, (float)(1.0 - bp2));
         const float lr = (tl < 3) ? p.lr_rot : p.lr_trans;
-        my_x -= lr * mh / (sqrtf(vh) + p.eps);
+        my_x -= __fdividef(lr * mh, sqrtf(vh) + p.eps);
       }
     }
 
@@ -926,7 +1030,7 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
     }
   }
 
-  if (MODE == MODE_MIN && p.stats != nullptr) {
+  if (MODE == MODE_MIN && STATS_REGS && p.stats != nullptr) {
     unsigned long long v[5] = {c_grid, c_look, c_ent, c_cpb, c_cpr};
 #pragma unroll
     for (int k = 0; k < 5; ++k) {

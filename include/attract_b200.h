@@ -97,9 +97,10 @@ typedef struct AttGrid {
   int nb_rec_bytes;            /* 32, 64 or 128: size of one neighbour record (below) */
   const float* pair;           /* [n_ltypes][n_rtypes][8], 32-B aligned: rc, ac, emin, rmin2, ivor, eplat, gplat, rcap2 */
   const void* nb_rec;          /* one neighbour record per list-grid point, 16-B aligned
-                                  (att_nbgrid_pack_records): u32 overflow index into nb_list, u16
-                                  count, then the first (nb_rec_bytes - 6) / 2 entries inline;
-                                  required with nb_hdr */
+                                  (att_nbgrid_pack_records): the first (nb_rec_bytes - 6) / 2
+                                  entries inline (u16 each, from byte 0), the u16 count at byte
+                                  nb_rec_bytes - 6, the u32 overflow index into nb_list at byte
+                                  nb_rec_bytes - 4; required with nb_hdr */
   int nb_refine;               /* 0 or 1: the lists sit at the inner grid points (the reference's
                                   neighbour grid); 2 or 4: at the points of the inner grid refined
                                   that many times per axis (spacing / r, (dim - 1) * r + 1 points per
@@ -282,8 +283,10 @@ int att_nbgrid_fill(const AttGridGeom* geom, const float* rec_dev, int n_rec, fl
                     const uint32_t* hdr_dev, uint16_t* list_dev, void* stream);
 
 /* Fixed-size neighbour records from the CSR lists: record v holds
-   {overflow index = start + inline, count, first `inline` entries (rest
-   ATT_NB_EMPTY)}; entries beyond the inline ones stay in the CSR list, which
+   {first `inline` entries (rest ATT_NB_EMPTY), count, overflow index = start
+   + inline} in the layout of AttGrid.nb_rec (entries first, so that the
+   kernels read four per 8-byte load); entries beyond the inline ones stay in
+   the CSR list, which
    the kernels keep reading.  A record is one bulk copy into shared memory,
    made when a bead's nearest inner grid point changes.
    records_dev: n_voxels * rec_bytes bytes, 16-B aligned; rec_bytes 32/64/128.

@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--launches", type=int, default=3, help="--profile-case: minimiser launches")
     ap.add_argument("--refine", type=int, default=4, help="--profile-case: neighbour-list grid refinement")
     ap.add_argument("--adam-steps", type=int, default=-1, help="--profile-case: ADAM steps (-1: the config's)")
+    ap.add_argument("--allpairs", action="store_true",
+                    help="--profile-case: the all-pairs rescoring kernel on config 3's receptor and ligand instead")
     return ap.parse_args()
 
 
@@ -580,6 +582,8 @@ def run_profile_case(args):
     from attract_b200 import synth
 
     A.load_library()
+    if args.allpairs:
+        return run_profile_allpairs(args)
     cfg = synth.make_config(args.config, seed=0, scale=args.scale, n_types=args.types, clustered=args.clustered)
     steps = cfg.steps if args.adam_steps < 0 else args.adam_steps
     grid = A.Grid.build(cfg.rec_xyz, cfg.rec_type, cfg.ff, cfg.geom, cutoff=cfg.cutoff, nb_refine=args.refine)
@@ -605,6 +609,33 @@ def run_profile_case(args):
     print(json.dumps({"config": args.config, "clustered": args.clustered, "scale": args.scale, "types": args.types,
                       "poses": wl.n_poses, "steps": steps, "lanes": lanes, "threads": shape.block_threads, "ms": ms,
                       "poses_per_s": wl.n_poses / ms * 1e3, "stats": st, "brick_gb": grid.bricks.numel() * 4 / 1e9}))
+
+
+def run_profile_allpairs(args):
+    """All-pairs rescoring with gradient of config 3's poses (scaled by
+    ``--scale``) on its 2500-bead receptor and 24-bead ligand, ``--launches``
+    times; prints the mean time of the launches after the first."""
+    import torch
+
+    from attract_b200 import synth
+    from attract_b200.allpairs import AllPairs
+
+    cfg = synth.make_config(3, seed=0, scale=args.scale, n_types=args.types)
+    xyz, _, lt = cfg.ligands[0]
+    ap = AllPairs(cfg.rec_xyz, cfg.rec_type, xyz, lt, cfg.ff)
+    P = torch.tensor(cfg.poses[0].astype(np.float32), device="cuda")
+    times = []
+    for _ in range(args.launches):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ap.energy(P, grad=True)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = float(np.mean(times[1:])) if len(times) > 1 else times[0]
+    pairs = len(cfg.rec_type) * len(xyz) * len(P)
+    print(json.dumps({"allpairs": True, "poses": len(P), "n_rec": len(cfg.rec_type), "n_lig": len(xyz), "ms": ms,
+                      "pairs_per_s": pairs / ms * 1e3, "poses_per_s": len(P) / ms * 1e3}))
 
 
 # --------------------------------------------------------------------------- reference

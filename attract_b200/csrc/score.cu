@@ -200,13 +200,14 @@ __device__ __forceinline__ int find_segment(const KParams& p, int tile) {
 // The bead's ligand type is valid here: phase A gives a bead list entries only
 // when its type is inside the pair table.  NE: accumulate the energy too (the
 // minimiser's steps before the last need only the gradient).
-template <bool NE>
+template <bool NE, bool REF>
 __device__ __forceinline__ void pair_term_masked(const KParams& p, const KGrid& G, const BeadPos& bp,
-                                                 const float4& r, float& e, float& gx, float& gy, float& gz) {
+                                                 const float4& r, bool jok, float& e, float& gx, float& gy,
+                                                 float& gz) {
   const float dx = bp.x - r.x, dy = bp.y - r.y, dz = bp.z - r.z;
   const float dsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   const int rt = __float_as_int(r.w);
-  const bool hit = (dsq < G.plateau2) & ((unsigned)rt < (unsigned)G.n_rtypes);
+  const bool hit = (dsq < G.plateau2) & ((unsigned)rt < (unsigned)G.n_rtypes) & jok;
   const int idx = hit ? bp.lt * G.n_rtypes + rt : 0;
   float4 p0, p1;  // rc, ac, emin, rmin2 / ivor, eplat, gplat, rcap2: one 32-B row
   ldg_f4x2(G.pair + (size_t)(unsigned)idx * 2, p0, p1);
@@ -224,7 +225,7 @@ __device__ __forceinline__ void pair_term_masked(const KParams& p, const KGrid& 
   const float dv2 = rr6 * rr2 * fmaf(-8.f * p0.x, rr2, 6.f * p0.y);
   float gm2 = near ? dv2 : p1.x * dv2;
   gm2 = (dsq < p1.w) ? 0.f : gm2;
-  if (p.grad_mode == ATT_GRAD_REFERENCE) gm2 = fmaf(-p1.z * G.plateau_x2, rsqrtf(dsq), gm2);
+  if (REF) gm2 = fmaf(-p1.z * G.plateau_x2, rsqrtf(dsq), gm2);
   const float gf = hit ? gm2 : 0.f;
   gx = gf * dx;
   gy = gf * dy;
@@ -265,6 +266,7 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
   uint32_t* pbuf = reinterpret_cast<uint32_t*>(nrec + 32 * K * (RS + 16 + ARM_BYTES));
   uint64_t* bar = reinterpret_cast<uint64_t*>(nrec + 32 * K * (RS + 16 + ARM_BYTES) + pair_buffer_bytes(K));
   const int tbase = slot * NB;  // this team's first bead record
+  const bool ref_grad = p.grad_mode == ATT_GRAD_REFERENCE;  // the pair loop and phase D compiled per mode
   uint32_t* pb = pbuf + slot * (PB + S);  // this team's pair buffer
 
   // Grid descriptors: copied from the parameters into shared memory with static
@@ -556,7 +558,7 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         biz[k] = (int)flz;
         bidx[k] = u ? gt * (int)G.type_stride + base + (bix[k] * (ny - 1) + biy[k]) * (nz - 1) + biz[k] : 0;
         nvox[k] = -1;
-        if (inn && G.nb_rec != nullptr && lt < G.n_ltypes) {
+        if (inn && G.nb_rec != nullptr && lt < G.n_ltypes && G.n_rec > 0) {
           // nearest list-grid point (the inner grid point itself when nb_scale = 1)
           const int nx = (int)floorf(fmaf(vx, G.nb_scale, 0.5f)), my = (int)floorf(fmaf(vy, G.nb_scale, 0.5f)),
                     mz = (int)floorf(fmaf(vz, G.nb_scale, 0.5f));
@@ -744,8 +746,9 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
           }
           __syncwarp();
           const unsigned n = min(team_total - min(team_total, q0), (unsigned)PB);
-          auto pair_window = [&](auto ne) {
+          auto pair_window = [&](auto ne, auto ref) {
           constexpr bool NE = decltype(ne)::value;
+          constexpr bool REF = decltype(ref)::value;
           for (unsigned s0 = tl; s0 < n; s0 += U * S) {
             unsigned ww[U];
 #pragma unroll
@@ -754,20 +757,25 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
               ww[m] = (s < n) ? pb[s] : (unsigned)ATT_NB_EMPTY;
             }
             float4 rr[U];
+            bool jok[U];
 #pragma unroll
             for (int m = 0; m < U; ++m) {
               const unsigned j = ww[m] & 0xffffu;
 #ifdef ATT_BOUNDS_CHECK
               if (j != ATT_NB_EMPTY) (void)ATT_CHECK(j < (unsigned)G.n_rec, 4, j, G.n_rec);
 #endif
-              rr[m] = (j < (unsigned)G.n_rec) ? ldg_f4(G.rec + j) : make_float4(1e15f, 1e15f, 1e15f, 0.f);
+              // an entry outside the receptor (the empty-slot sentinel) reads the last
+              // bead and is masked in the pair term (phase A gives beads list entries
+              // only when the receptor has beads)
+              jok[m] = j < (unsigned)G.n_rec;
+              rr[m] = ldg_f4(G.rec + min(j, (unsigned)G.n_rec - 1u));
             }
 #pragma unroll
             for (int m = 0; m < U; ++m) {
               const unsigned bi = tbase + (ww[m] >> 16);
               const BeadPos bp = bpos[bi];
               float px, py, pz;
-              pair_term_masked<NE>(p, G, bp, rr[m], acc_e, px, py, pz);
+              pair_term_masked<NE, REF>(p, G, bp, rr[m], jok[m], acc_e, px, py, pz);
               // moment arm: the bead position X (the torque about t, sum (X - t) x g,
               // is sum X x g - t x sum g, formed after the team sum); the
               // 4x4 form accumulates with the ligand-frame x
@@ -789,15 +797,21 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
             }
           }
           };
-          if (need_e) pair_window(std::true_type{});
-          else pair_window(std::false_type{});
+          if (ref_grad) {
+            if (need_e) pair_window(std::true_type{}, std::true_type{});
+            else pair_window(std::false_type{}, std::true_type{});
+          } else {
+            if (need_e) pair_window(std::true_type{}, std::false_type{});
+            else pair_window(std::false_type{}, std::false_type{});
+          }
           __syncwarp();  // the next window overwrites the buffer
         }
       }
 
       // ---------------- phase D: grid term from the bricks in shared memory
-      auto phase_d = [&](auto ne) {
+      auto phase_d = [&](auto ne, auto ref) {
       constexpr bool NE = decltype(ne)::value;
+      constexpr bool REF = decltype(ref)::value;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (use[k]) {
@@ -821,7 +835,7 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
             const float wx = (q & 4) ? wx1 : wx0, wy = (q & 2) ? wy1 : wy0, wz = (q & 1) ? wz1 : wz0;
             const float w = wx * wy * wz;
             if (NE) eb = fmaf(w, v.x, eb);
-            if (p.grad_mode == ATT_GRAD_REFERENCE) {
+            if (REF) {
               gbx = fmaf(-w, v.y, gbx);
               gby = fmaf(-w, v.z, gby);
               gbz = fmaf(-w, v.w, gbz);
@@ -869,8 +883,13 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         }
       }
       };
-      if (need_e) phase_d(std::true_type{});
-      else phase_d(std::false_type{});
+      if (ref_grad) {
+        if (need_e) phase_d(std::true_type{}, std::true_type{});
+        else phase_d(std::false_type{}, std::true_type{});
+      } else {
+        if (need_e) phase_d(std::true_type{}, std::false_type{});
+        else phase_d(std::false_type{}, std::false_type{});
+      }
       // the next chunk's / evaluation's bulk copies overwrite the slots read above
       __syncwarp();
       fence_proxy_async();

@@ -91,6 +91,27 @@ def test_dense_lists_many_pair_windows(n_beads, lanes):
     assert hdr[:, 1].max() > 64
 
 
+def test_empty_slot_sentinels_inside_lists_are_skipped():
+    """Lists given the reference's way may hold the empty-slot value 65535
+    inside a point's count (read_grid2.py:118, test5.py:240): such entries add
+    nothing, as in the oracle, at 1 and 2 beads per lane."""
+    A = _engine()
+    c = small_case(seed=42, n_poses=64, n_lig_beads=24)
+    hdr, lst = c["G"]["nb_hdr"], c["G"]["nb_list"].copy()
+    rng = np.random.default_rng(3)
+    hit = rng.random(len(lst)) < 0.2
+    lst[hit] = 65535
+    c["G"]["nb_list"] = lst
+    assert hit.sum() > 100 and hdr[:, 1].sum() == len(lst)
+    grid = to_device_grid(c)
+    for lanes in (32, 16):
+        wl = _wl(A, grid, c["lig"], c["gt"], c["lt"], len(c["poses"]), lanes)
+        E, G, S = A.energrad(wl, torch.tensor(c["poses"], dtype=torch.float32, device="cuda"))
+        Eo, Go = O.energrad(c["poses"], c["lig"], c["gt"], c["lt"], c["G"])
+        _check(f"sentinels in lists, {lanes} lanes", c, E.cpu().numpy(), G.cpu().numpy(), Eo, Go)
+        assert np.all(S.cpu().numpy() == 0)
+
+
 @pytest.mark.parametrize("lanes", [8, 32])
 def test_energy_only_equals_energy_with_gradient(lanes):
     """The reference's self-consistency check (energy-only and value-and-grad

@@ -36,7 +36,9 @@ _CACHE = {}
 
 
 def _config(idx):
-    """(cfg, grid, oracle grid dict) of configuration ``idx``, built once."""
+    """(cfg, grid, oracle grid dict) of configuration ``idx`` (``"2c"``: config
+    2 with the clustered receptor; ``"2c32"``: the same with 32-byte records,
+    so that most long lists continue in the CSR overflow), built once."""
     if idx in _CACHE:
         return _CACHE[idx]
     for k in list(_CACHE):  # one configuration's grids resident at a time
@@ -46,8 +48,12 @@ def _config(idx):
     A = _A()
     from attract_b200 import synth
 
-    cfg = synth.make_config(idx, seed=0)
+    clustered = idx in ("2c", "2c32")
+    cfg = synth.make_config(2 if clustered else idx, seed=0, clustered=clustered)
     grid = A.Grid.build(cfg.rec_xyz, cfg.rec_type, cfg.ff, cfg.geom, cutoff=cfg.cutoff, keep_dense=True)
+    if idx == "2c32":
+        grid._pack_records(32)
+        grid._att = None
     _CACHE[idx] = (cfg, grid, oracle_grid(grid, cfg.ff))
     return _CACHE[idx]
 
@@ -80,15 +86,19 @@ def sample(cfg, per_lig):
 _ORACLE = {}
 # grouped by configuration, so that each configuration's grids are built once
 ENERGRAD_CASES = [(idx, n, lanes, mode) for idx, n, shapes in ((0, 4096, (8, 32)), (1, 256, (32, 8)),
-                                                                (2, 2048, (32, 16)))
+                                                                (2, 2048, (32, 16)), ("2c", 2048, (32,)),
+                                                                ("2c32", 2048, (32,)))
                   for mode in ("reference", "analytic") for lanes in shapes]
 
 
 @pytest.mark.parametrize("idx,per_lig,lanes,mode", ENERGRAD_CASES)
 def test_config_energrad_vs_fp64(idx, per_lig, lanes, mode):
     """One energy + gradient evaluation of sampled configuration poses (config
-    0: all 4096; config 1: 256 per fragment; config 2: 2048 surface poses)
-    against the float64 oracle, at two launch shapes."""
+    0: all 4096; config 1: 256 per fragment; config 2: 2048 surface poses,
+    with the uniform and the clustered receptor, whose lists of up to ~80
+    entries take 128-byte records -- and, repacked into 32-byte records, run
+    far past the inline entries into the CSR overflow) against the float64
+    oracle, at one or two launch shapes."""
     A = _A()
     cfg, grid, G = _config(idx)
     parts = sample(cfg, per_lig)
@@ -125,7 +135,7 @@ def _rank_metrics(E, Eref):
     return out
 
 
-MIN_CASES = [(0, 1024, 8), (1, 64, 32), (2, 256, 32)]
+MIN_CASES = [(0, 1024, 8), (1, 64, 32), (2, 256, 32), ("2c", 256, 32)]
 
 
 @pytest.mark.parametrize("idx,per_lig,lanes", MIN_CASES)

@@ -22,7 +22,6 @@ ATT_MAX_GRIDS = 8
 ATT_KERR_COPY_TIMEOUT = 1
 ATT_KERR_BOUNDS = 2
 ATT_KERR_BAD_SEGMENT = 4
-ATT_TEST_STALL_COPY_WAIT = 1
 ATT_NB_EMPTY = 65535
 
 

@@ -202,7 +202,8 @@ static int fill_common(KParams* p, const AttGrid* grids, int n_grids, const AttL
     if (p->grid[i].nb_rec_bytes > rec_slot) rec_slot = p->grid[i].nb_rec_bytes;
   }
   p->rec_slot = rec_slot;
-  p->test_flags = launch ? launch->test_flags : 0;
+  REQUIRE(!launch || launch->test_flags == 0, "AttLaunchCfg.test_flags is reserved and must be 0");
+  p->test_flags = 0;
   if (!(launch && launch->block_threads)) {  // default: the largest block whose shared memory fits
     while (t > 32 && score_smem_bytes(*K, t, rec_slot) > kDynSmemLimit) t -= 32;
     *threads = t;

@@ -68,7 +68,7 @@ struct KParams {
   float lr_rot, lr_trans, b1, b2, eps;
   int step0;
   int rec_slot;          // bytes of a neighbour-record slot in shared memory (max over grids)
-  int test_flags;        // AttLaunchCfg.test_flags
+  int test_flags;        // reserved (0)
   int qs_n;               // MODE_QUAT: SCHEMA stages, epochs / learning rate / gravity on-off per stage
   int qs_epochs[ATT_MAX_STAGES];
   float qs_lr[ATT_MAX_STAGES];

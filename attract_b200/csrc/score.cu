@@ -6,12 +6,13 @@
 // evaluation of a pose runs in three phases:
 //
 //  A  every owner lane moves its beads, computes the voxel, and -- when its
-//     shared-memory slot does not already hold them -- bulk-copies (TMA
-//     engine) the bead's 128-byte grid brick (the 8 trilinear corners of the
-//     voxel, (E, Fx, Fy, Fz) each) and the fixed-size neighbour record of its
-//     nearest inner grid point into the warp's shared memory, completing on
-//     the warp's mbarrier.  A bead moves ~0.1 A per ADAM step against 0.9 A
-//     cells, so only a few percent of evaluations copy anything;
+//     shared-memory slot does not already hold them -- copies the bead's
+//     128-byte grid brick (the 8 trilinear corners of the voxel, (E, Fx, Fy,
+//     Fz) each) and the fixed-size neighbour record of its nearest list-grid
+//     point into its slots of the warp's shared memory (16-byte cp.async
+//     through L2, completed by the lane's own wait_group).  A bead moves
+//     ~0.1 A per ADAM step against 0.9 A cells, so only a few percent of
+//     evaluations copy anything;
 //  C  neighbour pairs: the owners write their beads' list entries into the
 //     team's pair buffer, and the team's lanes take the pairs round-robin
 //     (balanced whatever the per-bead list lengths);
@@ -22,8 +23,8 @@
 // so each lane accumulates its own share and the team sums 7 values with
 // xor-shuffles per evaluation.  The rigid-body ADAM step runs on team lanes
 // 0..5 between evaluations; a persistent launch pulls tiles of poses from a
-// work counter.  Every mbarrier wait is bounded; a timeout sets the device
-// error word and the warp returns.
+// work counter.  No thread waits on a flag, a barrier object or another
+// thread's copy: a lane waits only for its own cp.async copies.
 //
 // Semantics follow test5.py (sjdv1982/attract-jax):
 //   transform            [x,1] @ mat                    test5.py:315-317
@@ -43,61 +44,23 @@
 namespace att {
 
 // ---------------------------------------------------------------------------
-// shared memory / mbarrier / bulk-copy helpers
+// shared memory and copy helpers
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+// 16-byte global -> shared copy through L2 (cp.async.cg), completed by
+// cp.async.wait_group in the issuing thread; both addresses 16-B aligned.
+// Only a few percent of beads copy per step; each lane issues its own
+// copies, in parallel with the other lanes that copy (measured 3.8 % faster
+// on config 1 than one bulk copy per brick or record completing on a warp
+// mbarrier).
+__device__ __forceinline__ void cp16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
-
-__device__ __forceinline__ void mbar_fence_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}"
-               ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// global -> shared through the bulk-copy (TMA) engine, completing on `bar`
-// (bytes: a multiple of 16; both addresses 16-B aligned).  A 128-B brick is
-// one line: the engine moves it without L1 wavefronts, unlike 16-B per-lane
-// copies, which saturate L1TEX on this gather.
-__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-
-// orders this thread's generic-proxy shared-memory reads before later
-// async-proxy (bulk-copy) writes to the same bytes
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// A copy wait gives up after COPY_WAIT_NS of %globaltimer (read every 64
-// polls), or after WAIT_POLL_LIMIT polls, whichever comes first.
-constexpr unsigned long long COPY_WAIT_NS = 1000000000ull;  // 1 s
-constexpr unsigned WAIT_POLL_LIMIT = 1u << 26;
-
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
+__device__ __forceinline__ void cp_commit_wait() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
 // Loads with a fixed state space.  A list entry comes either from the
@@ -163,7 +126,7 @@ __device__ __noinline__ void bounds_report(int code, long long a, long long b) {
 // slot of rec_slot bytes, a 16-B moved-bead record and, in the modes that
 // accumulate dE/dmat, a 16-B ligand-frame record; the pair buffers of the
 // warp's teams (pairs_per_bead(K) u32 words per bead slot, plus S words of
-// padding per team so that teams start in different banks); the mbarrier.
+// padding per team so that teams start in different banks).
 // A team with more pairs than its buffer holds takes several windows; with
 // several beads per lane, 4 words per slot keep a block's shared memory small
 // enough for one more block per SM (13 % faster on 40-bead ligands at 2 beads
@@ -175,7 +138,7 @@ __host__ __device__ inline size_t pair_buffer_bytes(int K) { return (size_t)32 *
 // others take the lever arm from the bead record)
 __host__ __device__ inline size_t warp_smem_bytes(int K, int rec_slot, bool arms = true) {
   return (size_t)32 * K * (128 + rec_stride(rec_slot) + sizeof(BeadPos) + (arms ? sizeof(BeadArm) : 0)) +
-         pair_buffer_bytes(K) + 16;
+         pair_buffer_bytes(K);
 }
 
 template <int S>
@@ -264,7 +227,6 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
   BeadArm* barm = reinterpret_cast<BeadArm*>(nrec + 32 * K * (RS + 16));  // ACC9 modes only
   constexpr int ARM_BYTES = ACC9 ? 16 : 0;
   uint32_t* pbuf = reinterpret_cast<uint32_t*>(nrec + 32 * K * (RS + 16 + ARM_BYTES));
-  uint64_t* bar = reinterpret_cast<uint64_t*>(nrec + 32 * K * (RS + 16 + ARM_BYTES) + pair_buffer_bytes(K));
   const int tbase = slot * NB;  // this team's first bead record
   const bool ref_grad = p.grad_mode == ATT_GRAD_REFERENCE;  // the pair loop and phase D compiled per mode
   uint32_t* pb = pbuf + slot * (PB + S);  // this team's pair buffer
@@ -278,12 +240,6 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
     if (threadIdx.x == g) s_grid[g] = p.grid[g];
   __syncthreads();
 
-  if (lane == 0) {
-    mbar_init(bar, 1);
-    mbar_fence_init();
-  }
-  __syncwarp();
-  uint32_t parity = 0;
 
   // statistics (MODE_MIN): bead evaluations with a brick, list lookups, list
   // entries, brick copies, record copies
@@ -579,11 +535,9 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
           }
         }
       }
-      // One bulk copy per brick and per neighbour record whose slot does not
-      // already hold it (chunked ligands share the slots: always copy).  The
-      // mbarrier phase completes when lane 0 has arrived and all bytes have
-      // landed (copies may finish before the arrive); a warp whose slots are
-      // all current skips the copy round.
+      // A copy of each brick and neighbour record whose slot does not already
+      // hold it (chunked ligands share the slots: always copy); a warp whose
+      // slots are all current skips the copy round.
       if (multi) {
 #pragma unroll
         for (int k = 0; k < K; ++k) held_b[k] = held_v[k] = -1;
@@ -618,39 +572,30 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
           if (lane == 0 && w) atomicAdd(p.stats + slot_of[i], (unsigned long long)w);
         }
       }
-      const unsigned warp_bytes = __reduce_add_sync(0xffffffffu, my_bytes);
-      if (warp_bytes != 0) {
-        // test hook (ATT_TEST_STALL_COPY_WAIT): the warp serving tile 0 expects
-        // 16 bytes that no copy delivers, so its bounded wait runs out
-        const unsigned stall = ((p.test_flags & ATT_TEST_STALL_COPY_WAIT) && tile == 0) ? 16u : 0u;
-        if (lane == 0) mbar_arrive_expect_tx(bar, warp_bytes + stall);
-        __syncwarp();
+      // Each lane copies its own beads' bricks and records (16-byte cp.async
+      // through L2) and waits for its own copies: a slot is read only by the
+      // lane that owns it.  A few percent of beads copy per step, so the
+      // copies are issued by the lanes that need them in parallel.
+      if (__any_sync(0xffffffffu, my_bytes != 0u)) {
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const int sk = tbase + tl + k * S;
-          if (need_b[k]) {
-            bulk_copy(bricks + (size_t)sk * 8, G.bricks + (size_t)bidx[k] * 8, 128u, bar);
-            held_b[k] = bidx[k];
-          }
-          if (need_v[k]) {
-            bulk_copy(nrec + (size_t)sk * RS, G.nb_rec + (size_t)nvox[k] * G.nb_rec_bytes, (unsigned)G.nb_rec_bytes,
-                      bar);
-            held_v[k] = nvox[k];
-          }
+      for (int k = 0; k < K; ++k) {
+        const int sk = tbase + tl + k * S;
+        if (need_b[k]) {
+          const float4* src = G.bricks + (size_t)bidx[k] * 8;
+          float4* dst = bricks + (size_t)sk * 8;
+#pragma unroll 1
+          for (int c = 0; c < 8; ++c) cp16(dst + c, src + c);
+          held_b[k] = bidx[k];
         }
-        bool done = mbar_try_wait(bar, parity);
-        if (!done) {
-          const unsigned long long t0 = globaltimer_ns();
-          for (unsigned it = 1; !done && it < WAIT_POLL_LIMIT; ++it) {
-            done = mbar_try_wait(bar, parity);
-            if (!done && (it & 63u) == 0u && globaltimer_ns() - t0 > COPY_WAIT_NS) break;
-          }
+        if (need_v[k]) {
+          const unsigned char* src = G.nb_rec + (size_t)nvox[k] * G.nb_rec_bytes;
+          unsigned char* dst = nrec + (size_t)sk * RS;
+#pragma unroll 1
+          for (int c = 0; c < G.nb_rec_bytes; c += 16) cp16(dst + c, src + c);
+          held_v[k] = nvox[k];
         }
-        if (!__all_sync(0xffffffffu, done)) {
-          if (lane == 0) atomicOr(&g_kernel_error, ATT_KERR_COPY_TIMEOUT);
-          return;  // a bulk copy never completed: report and leave (whole warp)
-        }
-        parity ^= 1u;
+      }
+      cp_commit_wait();
       }
 
       // ---------------- phase C: neighbour pairs, balanced over the team.
@@ -890,9 +835,9 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         if (need_e) phase_d(std::true_type{}, std::false_type{});
         else phase_d(std::false_type{}, std::false_type{});
       }
-      // the next chunk's / evaluation's bulk copies overwrite the slots read above
+      // the next chunk's / evaluation's copies overwrite the slots read above
+      // (each lane its own slots, after its own reads)
       __syncwarp();
-      fence_proxy_async();
       }  // chunks
 
       // ---------------- team reduction and output / ADAM

@@ -60,7 +60,7 @@ class LaunchShape:
     lanes_per_pose: int = 8   # 8 / 16 / 32 lanes per pose = 4 / 2 / 1 poses per warp
     block_threads: int = 0    # 32, 64, 96 or 128; 0 = the largest that fits in shared memory
     blocks: int = 0           # persistent CTAs; 0 = fill the GPU
-    test_flags: int = 0       # ATT_TEST_* failure-path hooks (tests only)
+    test_flags: int = 0       # reserved: 0
 
     def to_c(self) -> _lib.AttLaunchCfg:
         c = _lib.AttLaunchCfg()

@@ -56,7 +56,8 @@ extern "C" {
 #define ATT_STATUS_NONFINITE_POSE 4   /* the input pose has a non-finite component */
 
 /* device-wide kernel error word (att_kernel_status) */
-#define ATT_KERR_COPY_TIMEOUT 1 /* a warp gave up waiting for its grid-brick / record bulk copies and returned */
+#define ATT_KERR_COPY_TIMEOUT 1 /* reserved: no kernel of this build waits on a copy, a flag or another thread
+                                   (a lane waits only for its own cp.async copies), so none can time out */
 #define ATT_KERR_BOUNDS 2       /* (ATT_BOUNDS_CHECK builds) an index failed its check; the access was skipped */
 #define ATT_KERR_BAD_SEGMENT 4  /* a segment named a missing grid or ligand or reached beyond n_pose_rows, or a
                                    pose's conformer index (pose_lig) or its ligand's bead range left the ligand
@@ -170,15 +171,9 @@ typedef struct AttLaunchCfg {
   int lanes_per_pose;   /* 8, 16 or 32 (poses per warp = 32 / lanes_per_pose) */
   int block_threads;    /* 32, 64, 96 or 128 (0 = the largest whose shared memory fits) */
   int blocks;           /* persistent CTAs (att_minimise), 0 = fill the GPU */
-  int test_flags;       /* 0; ATT_TEST_* bits exercise failure paths (tests only) */
+  int test_flags;       /* reserved: must be 0 */
 } AttLaunchCfg;
 
-/* AttLaunchCfg.test_flags: the warp serving tile 0 waits for 16 bytes that no
-   copy delivers.  Its bounded copy wait gives up after about a second, sets
-   ATT_KERR_COPY_TIMEOUT in the device error word and the warp returns (its
-   poses' outputs stay unwritten); the rest of the launch completes.  Lets a
-   test check the timeout path without hanging the GPU. */
-#define ATT_TEST_STALL_COPY_WAIT 1
 
 const char* att_last_error_string(void);
 const char* att_version(void);

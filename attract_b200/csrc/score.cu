@@ -10,9 +10,11 @@
 //     128-byte grid brick (the 8 trilinear corners of the voxel, (E, Fx, Fy,
 //     Fz) each) and the fixed-size neighbour record of its nearest list-grid
 //     point into its slots of the warp's shared memory (16-byte cp.async
-//     through L2, completed by the lane's own wait_group).  A bead moves
-//     ~0.1 A per ADAM step against 0.9 A cells, so only a few percent of
-//     evaluations copy anything;
+//     through L2, each lane's completed by its own wait_group: in the
+//     minimisers every lane copies for its own beads; the single-evaluation
+//     modes spread the warp's copies over all 32 lanes and end with a warp
+//     barrier).  A bead moves ~0.1 A per ADAM step against 0.9 A cells, so
+//     only a few percent of a minimisation's evaluations copy anything;
 //  C  neighbour pairs: the owners write their beads' list entries into the
 //     team's pair buffer, and the team's lanes take the pairs round-robin
 //     (balanced whatever the per-bead list lengths);
@@ -23,8 +25,8 @@
 // so each lane accumulates its own share and the team sums 7 values with
 // xor-shuffles per evaluation.  The rigid-body ADAM step runs on team lanes
 // 0..5 between evaluations; a persistent launch pulls tiles of poses from a
-// work counter.  No thread waits on a flag, a barrier object or another
-// thread's copy: a lane waits only for its own cp.async copies.
+// work counter.  No thread waits on a flag or a barrier object: a lane waits
+// only for its own cp.async copies and at warp barriers.
 //
 // Semantics follow test5.py (sjdv1982/attract-jax):
 //   transform            [x,1] @ mat                    test5.py:315-317
@@ -52,12 +54,16 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 
 // 16-byte global -> shared copy through L2 (cp.async.cg), completed by
 // cp.async.wait_group in the issuing thread; both addresses 16-B aligned.
-// Only a few percent of beads copy per step; each lane issues its own
-// copies, in parallel with the other lanes that copy (measured 3.8 % faster
-// on config 1 than one bulk copy per brick or record completing on a warp
-// mbarrier).
-__device__ __forceinline__ void cp16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+// (Measured against one bulk copy per brick or record completing on a warp
+// mbarrier: 3.8 % faster in the minimiser, per lane; 11 % faster for single
+// evaluations, spread over the warp.)
+__device__ __forceinline__ void cp16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
 }
 __device__ __forceinline__ void cp_commit_wait() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
@@ -146,6 +152,35 @@ __device__ __forceinline__ float team_sum(float v) {
 #pragma unroll
   for (int off = S / 2; off >= 1; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
   return v;
+}
+
+// Sums of six values over a 32-lane team, on every lane.  A reduce-scatter
+// butterfly: the first three levels each send half of the values still held
+// and keep the other half (lanes with the level's bit clear keep the first
+// half), so the six sums take 8 shuffles instead of 30; each sum is then
+// broadcast from the lanes that hold it (value i at lane 0, 8, 4, 16, 24,
+// 20).  Each sum is formed once, so every lane receives the same bits.
+__device__ __forceinline__ void warp_sum6(float& a0, float& a1, float& a2, float& a3, float& a4, float& a5,
+                                          int lane) {
+  constexpr unsigned F = 0xffffffffu;
+  const bool h4 = lane & 16, h3 = lane & 8, h2 = lane & 4;
+  float k0 = h4 ? a3 : a0, k1 = h4 ? a4 : a1, k2 = h4 ? a5 : a2;  // kept: (a0 a1 a2) or (a3 a4 a5)
+  k0 += __shfl_xor_sync(F, h4 ? a0 : a3, 16);
+  k1 += __shfl_xor_sync(F, h4 ? a1 : a4, 16);
+  k2 += __shfl_xor_sync(F, h4 ? a2 : a5, 16);
+  float m = h3 ? k1 : k0;  // kept: the first or the second of the three
+  m += __shfl_xor_sync(F, h3 ? k0 : k1, 8);
+  k2 += __shfl_xor_sync(F, k2, 8);
+  float r = h2 ? k2 : m;   // kept: that one, or the third
+  r += __shfl_xor_sync(F, h2 ? m : k2, 4);
+  r += __shfl_xor_sync(F, r, 2);
+  r += __shfl_xor_sync(F, r, 1);
+  a0 = __shfl_sync(F, r, 0);
+  a1 = __shfl_sync(F, r, 8);
+  a2 = __shfl_sync(F, r, 4);
+  a3 = __shfl_sync(F, r, 16);
+  a4 = __shfl_sync(F, r, 24);
+  a5 = __shfl_sync(F, r, 20);
 }
 
 __device__ __forceinline__ int find_segment(const KParams& p, int tile) {
@@ -543,12 +578,10 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         for (int k = 0; k < K; ++k) held_b[k] = held_v[k] = -1;
       }
       bool need_b[K], need_v[K];
-      unsigned my_bytes = 0;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         need_b[k] = use[k] && bidx[k] != held_b[k];
         need_v[k] = nvox[k] >= 0 && nvox[k] != held_v[k];
-        my_bytes += (need_b[k] ? 128u : 0u) + (need_v[k] ? (unsigned)G.nb_rec_bytes : 0u);
         if (MODE == MODE_MIN && STATS_REGS && want_stats) {
           c_grid += use[k] ? 1u : 0u;
           c_look += nvox[k] >= 0 ? 1u : 0u;
@@ -572,30 +605,85 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
           if (lane == 0 && w) atomicAdd(p.stats + slot_of[i], (unsigned long long)w);
         }
       }
-      // Each lane copies its own beads' bricks and records (16-byte cp.async
-      // through L2) and waits for its own copies: a slot is read only by the
-      // lane that owns it.  A few percent of beads copy per step, so the
-      // copies are issued by the lanes that need them in parallel.
-      if (__any_sync(0xffffffffu, my_bytes != 0u)) {
+      // The minimisers copy for a few percent of their beads per step: each lane
+      // that needs a brick or record copies it (16-byte cp.async through L2,
+      // in parallel with the other lanes that copy) and waits for its own
+      // copies, and only the owner reads a slot.  The single-evaluation modes
+      // copy for nearly every bead: the warp's copies are listed as (source
+      // index, bead slot) in the pair buffer (unused until phase C) and spread
+      // over all 32 lanes, consecutive lanes copying consecutive 16-byte chunks
+      // of one brick or record, so that a copy instruction fills whole 128-byte
+      // lines instead of one chunk of 32 lines; each lane waits for its own
+      // copies, and the warp barrier after the wait hands every slot to its
+      // owner.  (Listing in the minimisers costs them registers and spills:
+      // 14 % slower on config 1; one chunk of 32 lines per instruction costs
+      // the single-evaluation modes a factor 1.9.)  The grid is warp-uniform:
+      // a warp's teams share one segment.
+      if constexpr (MODE == MODE_MIN || QUAT) {
+        unsigned my_bytes = 0;
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const int sk = tbase + tl + k * S;
-        if (need_b[k]) {
-          const float4* src = G.bricks + (size_t)bidx[k] * 8;
-          float4* dst = bricks + (size_t)sk * 8;
+        for (int k = 0; k < K; ++k) my_bytes |= (need_b[k] ? 1u : 0u) | (need_v[k] ? 1u : 0u);
+        if (__any_sync(0xffffffffu, my_bytes != 0u)) {
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const unsigned sk = (unsigned)(tbase + tl + k * S);
+            if (need_b[k]) {
+              const char* src = reinterpret_cast<const char*>(G.bricks + (size_t)bidx[k] * 8);
+              const uint32_t dst = smem_u32(bricks) + sk * 128u;
 #pragma unroll 1
-          for (int c = 0; c < 8; ++c) cp16(dst + c, src + c);
-          held_b[k] = bidx[k];
-        }
-        if (need_v[k]) {
-          const unsigned char* src = G.nb_rec + (size_t)nvox[k] * G.nb_rec_bytes;
-          unsigned char* dst = nrec + (size_t)sk * RS;
+              for (unsigned c = 0; c < 128u; c += 16u) cp16(dst + c, src + c);
+              held_b[k] = bidx[k];
+            }
+            if (need_v[k]) {
+              const unsigned char* src = G.nb_rec + (size_t)nvox[k] * G.nb_rec_bytes;
+              const uint32_t dst = smem_u32(nrec) + sk * (unsigned)RS;
 #pragma unroll 1
-          for (int c = 0; c < G.nb_rec_bytes; c += 16) cp16(dst + c, src + c);
-          held_v[k] = nvox[k];
+              for (unsigned c = 0; c < (unsigned)G.nb_rec_bytes; c += 16u) cp16(dst + c, src + c);
+              held_v[k] = nvox[k];
+            }
+          }
+          cp_commit_wait();
         }
-      }
-      cp_commit_wait();
+      } else {
+        uint2* list_b = reinterpret_cast<uint2*>(pbuf);  // [32K] bricks
+        uint2* list_v = list_b + 32 * K;                 // [32K] records
+        unsigned nb_cp = 0, nv_cp = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const unsigned sk = (unsigned)(tbase + tl + k * S);
+          const unsigned mb = __ballot_sync(0xffffffffu, need_b[k]);
+          const unsigned mv = __ballot_sync(0xffffffffu, need_v[k]);
+          if (need_b[k]) {
+            list_b[nb_cp + __popc(mb & lanemask_lt())] = make_uint2((unsigned)bidx[k], sk);
+            held_b[k] = bidx[k];
+          }
+          if (need_v[k]) {
+            list_v[nv_cp + __popc(mv & lanemask_lt())] = make_uint2((unsigned)nvox[k], sk);
+            held_v[k] = nvox[k];
+          }
+          nb_cp += __popc(mb);
+          nv_cp += __popc(mv);
+        }
+        if (nb_cp + nv_cp != 0u) {
+          __syncwarp();
+          const char* gb = reinterpret_cast<const char*>(G.bricks);
+          for (unsigned i = lane; i < nb_cp * 8u; i += 32u) {
+            const uint2 e = list_b[i >> 3];
+            const unsigned c = (i & 7u) * 16u;
+            cp16(smem_u32(bricks) + e.y * 128u + c, gb + ((size_t)e.x * 128u + c));
+          }
+          if (nv_cp != 0u) {
+            const unsigned RB = (unsigned)G.nb_rec_bytes;  // 32, 64 or 128
+            const int rsh = __ffs(RB) - 5;                 // log2 of the 16-byte chunks per record
+            for (unsigned i = lane; i < (nv_cp << rsh); i += 32u) {
+              const uint2 e = list_v[i >> rsh];
+              const unsigned c = (i & ((1u << rsh) - 1u)) * 16u;
+              cp16(smem_u32(nrec) + e.y * (unsigned)RS + c, G.nb_rec + ((size_t)e.x * RB + c));
+            }
+          }
+          cp_commit_wait();
+          __syncwarp();
+        }
       }
 
       // ---------------- phase C: neighbour pairs, balanced over the team.
@@ -835,18 +923,22 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         if (need_e) phase_d(std::true_type{}, std::false_type{});
         else phase_d(std::false_type{}, std::false_type{});
       }
-      // the next chunk's / evaluation's copies overwrite the slots read above
-      // (each lane its own slots, after its own reads)
+      // the next chunk's / evaluation's copies (by any lane of the warp)
+      // overwrite the slots read above
       __syncwarp();
       }  // chunks
 
       // ---------------- team reduction and output / ADAM
       if (need_e) acc_e = team_sum<S>(acc_e);
-      acc_gx = team_sum<S>(acc_gx);
-      acc_gy = team_sum<S>(acc_gy);
-      acc_gz = team_sum<S>(acc_gz);
+      if constexpr (S == 32 && !ACC9) {
+        warp_sum6(acc_gx, acc_gy, acc_gz, acc_t[0], acc_t[1], acc_t[2], lane);
+      } else {
+        acc_gx = team_sum<S>(acc_gx);
+        acc_gy = team_sum<S>(acc_gy);
+        acc_gz = team_sum<S>(acc_gz);
 #pragma unroll
-      for (int k = 0; k < (ACC9 ? 9 : 3); ++k) acc_t[k] = team_sum<S>(acc_t[k]);
+        for (int k = 0; k < (ACC9 ? 9 : 3); ++k) acc_t[k] = team_sum<S>(acc_t[k]);
+      }
       if (!ACC9) {  // torque about the pose's translation: sum X x g - t x sum g
         acc_t[0] -= fmaf(ty, acc_gz, -tz * acc_gy);
         acc_t[1] -= fmaf(tz, acc_gx, -tx * acc_gz);

@@ -154,33 +154,39 @@ __device__ __forceinline__ float team_sum(float v) {
   return v;
 }
 
-// Sums of six values over a 32-lane team, on every lane.  A reduce-scatter
-// butterfly: the first three levels each send half of the values still held
-// and keep the other half (lanes with the level's bit clear keep the first
-// half), so the six sums take 8 shuffles instead of 30; each sum is then
-// broadcast from the lanes that hold it (value i at lane 0, 8, 4, 16, 24,
-// 20).  Each sum is formed once, so every lane receives the same bits.
-__device__ __forceinline__ void warp_sum6(float& a0, float& a1, float& a2, float& a3, float& a4, float& a5,
+// Sums of six values over a team of S lanes, on every lane of the team.  A
+// reduce-scatter butterfly: the first three levels (lane bits S/2, S/4, S/8)
+// each send half of the values still held and keep the other half (a lane
+// with the level's bit clear keeps the first half), the remaining levels sum
+// the one value left, so the six sums take 8 / 7 / 6 shuffles at S = 32 /
+// 16 / 8 instead of 30 / 24 / 18; each sum is then broadcast from the lanes
+// that hold it (team lane 0, S/4, S/8, S/2, S/2 + S/4, S/2 + S/8).  Each sum
+// is formed once, so every lane receives the same bits.
+template <int S>
+__device__ __forceinline__ void team_sum6(float& a0, float& a1, float& a2, float& a3, float& a4, float& a5,
                                           int lane) {
+  static_assert(S >= 8, "three scatter levels");
   constexpr unsigned F = 0xffffffffu;
-  const bool h4 = lane & 16, h3 = lane & 8, h2 = lane & 4;
-  float k0 = h4 ? a3 : a0, k1 = h4 ? a4 : a1, k2 = h4 ? a5 : a2;  // kept: (a0 a1 a2) or (a3 a4 a5)
-  k0 += __shfl_xor_sync(F, h4 ? a0 : a3, 16);
-  k1 += __shfl_xor_sync(F, h4 ? a1 : a4, 16);
-  k2 += __shfl_xor_sync(F, h4 ? a2 : a5, 16);
-  float m = h3 ? k1 : k0;  // kept: the first or the second of the three
-  m += __shfl_xor_sync(F, h3 ? k0 : k1, 8);
-  k2 += __shfl_xor_sync(F, k2, 8);
-  float r = h2 ? k2 : m;   // kept: that one, or the third
-  r += __shfl_xor_sync(F, h2 ? m : k2, 4);
-  r += __shfl_xor_sync(F, r, 2);
-  r += __shfl_xor_sync(F, r, 1);
-  a0 = __shfl_sync(F, r, 0);
-  a1 = __shfl_sync(F, r, 8);
-  a2 = __shfl_sync(F, r, 4);
-  a3 = __shfl_sync(F, r, 16);
-  a4 = __shfl_sync(F, r, 24);
-  a5 = __shfl_sync(F, r, 20);
+  constexpr int H1 = S / 2, H2 = S / 4, H3 = S / 8;
+  const bool h1 = lane & H1, h2 = lane & H2, h3 = lane & H3;
+  float k0 = h1 ? a3 : a0, k1 = h1 ? a4 : a1, k2 = h1 ? a5 : a2;  // kept: (a0 a1 a2) or (a3 a4 a5)
+  k0 += __shfl_xor_sync(F, h1 ? a0 : a3, H1);
+  k1 += __shfl_xor_sync(F, h1 ? a1 : a4, H1);
+  k2 += __shfl_xor_sync(F, h1 ? a2 : a5, H1);
+  float m = h2 ? k1 : k0;  // kept: the first or the second of the three
+  m += __shfl_xor_sync(F, h2 ? k0 : k1, H2);
+  k2 += __shfl_xor_sync(F, k2, H2);
+  float r = h3 ? k2 : m;   // kept: that one, or the third
+  r += __shfl_xor_sync(F, h3 ? m : k2, H3);
+#pragma unroll
+  for (int off = H3 / 2; off >= 1; off >>= 1) r += __shfl_xor_sync(F, r, off);
+  const int lead = lane & ~(S - 1);
+  a0 = __shfl_sync(F, r, lead);
+  a1 = __shfl_sync(F, r, lead + H2);
+  a2 = __shfl_sync(F, r, lead + H3);
+  a3 = __shfl_sync(F, r, lead + H1);
+  a4 = __shfl_sync(F, r, lead + H1 + H2);
+  a5 = __shfl_sync(F, r, lead + H1 + H3);
 }
 
 __device__ __forceinline__ int find_segment(const KParams& p, int tile) {
@@ -630,15 +636,26 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
             if (need_b[k]) {
               const char* src = reinterpret_cast<const char*>(G.bricks + (size_t)bidx[k] * 8);
               const uint32_t dst = smem_u32(bricks) + sk * 128u;
+              if constexpr (K == 1) {  // (unrolled, more beads per lane would spill)
+#pragma unroll
+                for (unsigned c = 0; c < 128u; c += 16u) cp16(dst + c, src + c);
+              } else {
 #pragma unroll 1
-              for (unsigned c = 0; c < 128u; c += 16u) cp16(dst + c, src + c);
+                for (unsigned c = 0; c < 128u; c += 16u) cp16(dst + c, src + c);
+              }
               held_b[k] = bidx[k];
             }
             if (need_v[k]) {
               const unsigned char* src = G.nb_rec + (size_t)nvox[k] * G.nb_rec_bytes;
               const uint32_t dst = smem_u32(nrec) + sk * (unsigned)RS;
+              unsigned c0 = 0;
+              if constexpr (K == 1) {  // records hold 32, 64 or 128 bytes
+                cp16(dst, src);
+                cp16(dst + 16u, src + 16);
+                c0 = 32u;
+              }
 #pragma unroll 1
-              for (unsigned c = 0; c < (unsigned)G.nb_rec_bytes; c += 16u) cp16(dst + c, src + c);
+              for (unsigned c = c0; c < (unsigned)G.nb_rec_bytes; c += 16u) cp16(dst + c, src + c);
               held_v[k] = nvox[k];
             }
           }
@@ -739,17 +756,19 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
                 const unsigned char* rk = nrec + (size_t)(tbase + tl + k * S) * RS;
                 const uint2 w = lds_u64(rk + 2 * c);
                 const unsigned tag = (unsigned)(tl + k * S) << 16;
-                const unsigned v4[4] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16};
+                // (receptor bead | bead slot << 16): one byte permute per entry
+                const unsigned v4[4] = {__byte_perm(w.x, tag, 0x7610), __byte_perm(w.x, tag, 0x7632),
+                                        __byte_perm(w.y, tag, 0x7610), __byte_perm(w.y, tag, 0x7632)};
                 if (one_window) {
                   uint32_t* dst = pb + (r + c);
 #pragma unroll
                   for (int i = 0; i < 4; ++i)
-                    if (c + i < nin) dst[i] = v4[i] | tag;
+                    if (c + i < nin) dst[i] = v4[i];
                 } else {
 #pragma unroll
                   for (int i = 0; i < 4; ++i) {
                     const unsigned pos = r + c + i - q0;
-                    if ((c + i < nin) & (pos < (unsigned)PB)) pb[pos] = v4[i] | tag;
+                    if ((c + i < nin) & (pos < (unsigned)PB)) pb[pos] = v4[i];
                   }
                 }
               }
@@ -930,8 +949,8 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
 
       // ---------------- team reduction and output / ADAM
       if (need_e) acc_e = team_sum<S>(acc_e);
-      if constexpr (S == 32 && !ACC9) {
-        warp_sum6(acc_gx, acc_gy, acc_gz, acc_t[0], acc_t[1], acc_t[2], lane);
+      if constexpr (!ACC9 && (K == 1 || S == 32)) {
+        team_sum6<S>(acc_gx, acc_gy, acc_gz, acc_t[0], acc_t[1], acc_t[2], lane);
       } else {
         acc_gx = team_sum<S>(acc_gx);
         acc_gy = team_sum<S>(acc_gy);
@@ -1058,7 +1077,9 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         const float mh = __fdividef(my_m, (float)(1.0 - bp1));
         const float vh = __fdividef(my_v, (float)(1.0 - bp2));
         const float lr = (tl < 3) ? p.lr_rot : p.lr_trans;
-        my_x -= __fdividef(lr * mh, sqrtf(vh) + p.eps);
+        float sv;  // approximate square root (the update's divisions are approximate too)
+        asm("sqrt.approx.f32 %0, %1;" : "=f"(sv) : "f"(vh));
+        my_x -= __fdividef(lr * mh, sv + p.eps);
       }
     }
 

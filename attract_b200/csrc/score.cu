@@ -229,7 +229,11 @@ __device__ __forceinline__ void pair_term_masked(const KParams& p, const KGrid& 
   const float dv2 = rr6 * rr2 * fmaf(-8.f * p0.x, rr2, 6.f * p0.y);
   float gm2 = near ? dv2 : p1.x * dv2;
   gm2 = (dsq < p1.w) ? 0.f : gm2;
-  if (REF) gm2 = fmaf(-p1.z * G.plateau_x2, rsqrtf(dsq), gm2);
+  if (REF) {  // the plateau shift's gradient, 1/d with a flush-to-zero approximate rsqrt
+    float rd;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rd) : "f"(dsq));
+    gm2 = fmaf(-p1.z * G.plateau_x2, rd, gm2);
+  }
   const float gf = hit ? gm2 : 0.f;
   gx = gf * dx;
   gy = gf * dy;

@@ -92,11 +92,6 @@ __device__ __forceinline__ uint4 lds_u128(const void* p) {  // p 16-byte aligned
                : "r"(smem_u32(p)) : "memory");
   return v;
 }
-__device__ __forceinline__ uint2 lds_u64(const void* p) {  // p 8-byte aligned
-  uint2 v;
-  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(smem_u32(p)) : "memory");
-  return v;
-}
 
 __device__ __forceinline__ unsigned ldg_nc_u16(const uint16_t* p) {
   unsigned short v;
@@ -754,44 +749,36 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         const unsigned warp_in = __reduce_max_sync(0xffffffffu, my_in);  // longest inline run of the warp
         const bool any_ovf = __any_sync(0xffffffffu, my_ovf);
         for (unsigned q0 = 0; q0 < warp_max; q0 += PB) {
-          // inline entries, EPL per shared load (8 per 16-byte load at one bead
-          // per lane: the 48-byte record stride keeps each quarter-warp phase
-          // free of bank conflicts; 4 per 8-byte load with more beads per lane,
-          // whose registers are short); a team whose pairs fit one window (the
-          // common case) needs no window test per entry
+          // inline entries, eight per 16-byte shared load (at the 48-byte
+          // stride of 32-byte records each quarter-warp phase is free of bank
+          // conflicts); a team whose pairs fit one window (the common case)
+          // needs no window test per entry
           const bool one_window = warp_max <= (unsigned)PB;
-          constexpr unsigned EPL = K == 1 ? 8u : 4u;
-          for (unsigned c = 0; c < warp_in; c += EPL) {
+          for (unsigned c = 0; c < warp_in; c += 8) {
             unsigned r = run0;
 #pragma unroll
             for (int k = 0; k < K; ++k) {
               const unsigned nin = min(ck[k], ninl);
               if (c < nin) {
                 const unsigned char* rk = nrec + (size_t)(tbase + tl + k * S) * RS;
-                unsigned w[EPL / 2];
-                if constexpr (EPL == 8) {
-                  const uint4 q = lds_u128(rk + 2 * c);
-                  w[0] = q.x; w[1] = q.y; w[2] = q.z; w[3] = q.w;
-                } else {
-                  const uint2 q = lds_u64(rk + 2 * c);
-                  w[0] = q.x; w[1] = q.y;
-                }
+                const uint4 q = lds_u128(rk + 2 * c);
+                const unsigned w[4] = {q.x, q.y, q.z, q.w};
                 const unsigned tag = (unsigned)(tl + k * S) << 16;
                 // (receptor bead | bead slot << 16): one byte permute per entry
-                unsigned v[EPL];
+                unsigned v[8];
 #pragma unroll
-                for (unsigned i = 0; i < EPL / 2; ++i) {
+                for (unsigned i = 0; i < 4; ++i) {
                   v[2 * i] = __byte_perm(w[i], tag, 0x7610);
                   v[2 * i + 1] = __byte_perm(w[i], tag, 0x7632);
                 }
                 if (one_window) {
                   uint32_t* dst = pb + (r + c);
 #pragma unroll
-                  for (unsigned i = 0; i < EPL; ++i)
+                  for (unsigned i = 0; i < 8; ++i)
                     if (c + i < nin) dst[i] = v[i];
                 } else {
 #pragma unroll
-                  for (unsigned i = 0; i < EPL; ++i) {
+                  for (unsigned i = 0; i < 8; ++i) {
                     const unsigned pos = r + c + i - q0;
                     if ((c + i < nin) & (pos < (unsigned)PB)) pb[pos] = v[i];
                   }

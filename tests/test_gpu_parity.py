@@ -58,6 +58,33 @@ def test_energrad_small_grid(mode, lanes):
     assert np.all(S.cpu().numpy() == 0)
 
 
+@pytest.mark.parametrize("lanes", [8, 32])
+def test_euler_angles_far_from_zero(lanes):
+    """The rotation's sines and cosines away from small angles: Euler angles
+    at and near multiples of pi/2, shifted by up to 1000 turns, and beyond
+    8192 rad (where the kernel's own reduction hands over to sincosf).  The
+    oracle takes sin/cos in float64 of the same float32 angles."""
+    A = _engine()
+    c = small_case(seed=7, n_poses=96)
+    rng = np.random.default_rng(7)
+    poses = c["poses"].astype(np.float32).copy()
+    n = len(poses)
+    quarter = rng.integers(-8, 9, (n, 3)) * (np.pi / 2) + rng.choice([0.0, 1e-6, -3e-4, 0.25], (n, 3))
+    turns = rng.integers(-1000, 1001, (n, 3)) * (2 * np.pi)
+    far = rng.uniform(8192.0, 30000.0, (n, 3)) * rng.choice([-1.0, 1.0], (n, 3))
+    group = np.arange(n) % 3
+    ang = np.where(group[:, None] == 0, quarter, np.where(group[:, None] == 1, poses[:, :3] + turns, far))
+    poses[:, :3] = ang.astype(np.float32)
+    grid = to_device_grid(c)
+    wl = _wl(A, grid, c["lig"], c["gt"], c["lt"], n, lanes)
+    E, G, S = A.energrad(wl, torch.tensor(poses, device="cuda"))
+    torch.cuda.synchronize()
+    P = poses.astype(np.float64)
+    Eo, Go = O.energrad(P, c["lig"], c["gt"], c["lt"], c["G"])
+    _check(f"Euler angles far from zero, {lanes} lanes", c, E.cpu().numpy(), G.cpu().numpy(), Eo, Go, poses=P)
+    assert np.all(S.cpu().numpy() == 0)
+
+
 def test_energrad_branches_ivor_nocap_gravity():
     """Uncapped potentials with repulsive (ivor=-1) pairs: clashes reach 1e10
     kcal/mol, where float32 position rounding dominates (the bound's input

@@ -56,8 +56,9 @@ extern "C" {
 #define ATT_STATUS_NONFINITE_POSE 4   /* the input pose has a non-finite component */
 
 /* device-wide kernel error word (att_kernel_status) */
-#define ATT_KERR_COPY_TIMEOUT 1 /* reserved: no kernel of this build waits on a copy, a flag or another thread
-                                   (a lane waits only for its own cp.async copies), so none can time out */
+#define ATT_KERR_COPY_TIMEOUT 1 /* reserved: no kernel of this build waits on a flag or another thread (a
+                                   lane waits only for its own cp.async copies and at warp barriers), so
+                                   none can time out */
 #define ATT_KERR_BOUNDS 2       /* (ATT_BOUNDS_CHECK builds) an index failed its check; the access was skipped */
 #define ATT_KERR_BAD_SEGMENT 4  /* a segment named a missing grid or ligand or reached beyond n_pose_rows, or a
                                    pose's conformer index (pose_lig) or its ligand's bead range left the ligand
@@ -280,10 +281,10 @@ int att_nbgrid_fill(const AttGridGeom* geom, const float* rec_dev, int n_rec, fl
 /* Fixed-size neighbour records from the CSR lists: record v holds
    {first `inline` entries (rest ATT_NB_EMPTY), count, overflow index = start
    + inline} in the layout of AttGrid.nb_rec (entries first, so that the
-   kernels read four per 8-byte load); entries beyond the inline ones stay in
-   the CSR list, which
-   the kernels keep reading.  A record is one bulk copy into shared memory,
-   made when a bead's nearest inner grid point changes.
+   kernels read eight per 16-byte load); entries beyond the inline ones stay
+   in the CSR list, which the kernels keep reading.  A record is copied into
+   shared memory (16-byte cp.async pieces) when a bead's nearest list-grid
+   point changes.
    records_dev: n_voxels * rec_bytes bytes, 16-B aligned; rec_bytes 32/64/128.
    (No counterpart in the reference: a layout of the neighbour grid of
    read_grid2.py:113-124 for the B200 kernels.) */

@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=120.0,
                     help="length of the serving run (0 = skip; the full serving workload is 600 s)")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="request arrivals per second")
+    ap.add_argument("--serve-round-steps", type=int, default=50,
+                    help="ADAM steps per serving round (a divisor of the 200 steps of a request)")
     ap.add_argument("--profile-case", action="store_true",
                     help="run only the minimiser on one configuration, --launches times (for ncu captures)")
     ap.add_argument("--config", type=int, default=1, help="--profile-case: configuration (0, 1 or 2)")
@@ -367,7 +369,7 @@ def other_configs(args, device, shape):
 
 def serving_run(args, device):
     """Four resident receptors, Poisson arrivals, lognormal pose counts,
-    continuous batching in rounds of 25 ADAM steps (200 per request).  Run
+    continuous batching in rounds of 50 ADAM steps (200 per request).  Run
     at the workload's arrival rate and, when that overloads the GPU, again at
     60% of the throughput it sustained, where p50/p99 describe a stable queue."""
     import torch
@@ -383,12 +385,14 @@ def serving_run(args, device):
     pool = np.concatenate([random_rotations(400_000, rng), random_in_ball(400_000, 30.0, rng)], 1).astype(np.float32)
     draw = lambda n: pool[(o := int(rng.integers(0, len(pool) - n))):o + n]
     desc = ("4 resident receptors (1500/3000/4500/6000 beads), ligands U{5..60} beads, poses lognormal(median "
-            "10000, sigma 1.0) clipped to [1000, 200000], 200 ADAM steps in rounds of 25; each round one launch "
+            f"10000, sigma 1.0) clipped to [1000, 200000], 200 ADAM steps in rounds of {args.serve_round_steps}; "
+            "each round one launch "
             "per launch shape (lanes per pose 8/16/32 and beads per lane by ligand size), rounds pipelined two "
             "deep, a pool of up to 2 M poses in flight")
 
     def one(rate, seconds):
-        srv = DockingServer(grids, steps=200, round_steps=25, max_inflight_poses=2_000_000, hbm_budget_bytes=150e9)
+        srv = DockingServer(grids, steps=200, round_steps=args.serve_round_steps, max_inflight_poses=2_000_000,
+                            hbm_budget_bytes=150e9)
         reqs = synth.serving_requests(int(seconds * rate * 1.5) + 10, seed=0, rate=rate)
         st = replay(srv, reqs, duration=seconds, pose_source=draw)
         offered = sum(q["n_poses"] for q in reqs if q["t"] <= seconds) / seconds

@@ -23,6 +23,7 @@
 //  C  neighbour pairs: the owners write their beads' list entries into the
 //     team's pair buffer, and the team's lanes take the pairs round-robin
 //     (balanced whatever the per-bead list lengths).
+// The adjoint (K2) runs C before D, which measured faster for its grid scatter.
 //
 // Energy, dE/dt and the torque are linear in every corner / pair contribution,
 // so each lane accumulates its own share and the team sums 7 values with
@@ -806,15 +807,22 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
         }
       }
       };
-      if (ref_grad) {
-        if (need_e) phase_d(std::true_type{}, std::true_type{});
-        else phase_d(std::false_type{}, std::true_type{});
-      } else {
-        if (need_e) phase_d(std::true_type{}, std::false_type{});
-        else phase_d(std::false_type{}, std::false_type{});
-      }
+      auto run_d = [&]() {
+        if (ref_grad) {
+          if (need_e) phase_d(std::true_type{}, std::true_type{});
+          else phase_d(std::false_type{}, std::true_type{});
+        } else {
+          if (need_e) phase_d(std::true_type{}, std::false_type{});
+          else phase_d(std::false_type{}, std::false_type{});
+        }
+      };
+      // Phase D runs first except in the adjoint, whose grid scatter runs after
+      // the pair term (measured on a 65 536-pose backward: 0.454 ms against
+      // 0.496 ms with phase D first; the forward modes gain 2 % with it first).
+      if constexpr (MODE != MODE_BWD) run_d();
       // the minimisers: this lane's records have landed
       if constexpr (MODE == MODE_MIN || QUAT) cp_wait<0>();
+      auto phase_c = [&]() {
 
       // ---------------- phase C: neighbour pairs, balanced over the team.
       // C1: every owner lane writes its beads' list entries (inline ones from
@@ -979,6 +987,9 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
           __syncwarp();  // the next window overwrites the buffer
         }
       }
+      };
+      phase_c();
+      if constexpr (MODE == MODE_BWD) run_d();
 
       // the next chunk's / evaluation's copies (by any lane of the warp)
       // overwrite the slots read above

@@ -254,8 +254,8 @@ __device__ __forceinline__ void pair_term_masked(const KParams& p, const KGrid& 
 
 // Blocks of 128 threads per SM: one bead per lane with 32-lane teams runs 6
 // (80 registers, one pair in flight per lane), with 8/16-lane teams 5 (their
-// minimiser would spill at 80); two beads per lane 4, more 2.  Measured on the
-// 18-30-bead config-1 mix: 6 blocks with one pair in flight beat 5 blocks with
+// minimiser would spill at 80); two beads per lane 4, more 2.  Measured on
+// 18-30-bead ligands against a 2500-bead receptor: 6 blocks with one pair in flight beat 5 blocks with
 // two by 6 %; with two beads per lane, one pair in flight lost 7-14 %.
 template <int S, int K>
 __host__ __device__ constexpr int score_blocks_per_sm() { return K == 1 ? (S == 32 ? 6 : 5) : K == 2 ? 4 : 2; }
@@ -632,7 +632,8 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
       // in parallel with the other lanes that copy) and waits for its own
       // copies, and only the owner reads a slot.  Bricks and records are
       // committed as two groups: phase D waits for the first, phase C after it
-      // for the second (measured: 3.6 % faster on config 1, 3.8 % on config 2,
+      // for the second (measured: 3.6 % faster on 18-30-bead ligands against a
+      // 2500-bead receptor, 3.8 % on a 40-bead ligand against 5000 beads,
       // and the two phases' values no longer share live registers: the
       // 32-lane minimiser's spills fell from 20 to 4 bytes).  The single-evaluation modes
       // copy for nearly every bead: the warp's copies are listed as (source
@@ -642,7 +643,7 @@ __global__ void __launch_bounds__(128, (score_blocks_per_sm<S, K>())) score_kern
       // lines instead of one chunk of 32 lines; each lane waits for its own
       // copies, and the warp barrier after the wait hands every slot to its
       // owner.  (Listing in the minimisers costs them registers and spills:
-      // 14 % slower on config 1; one chunk of 32 lines per instruction costs
+      // 14 % slower on 18-30-bead ligands; one chunk of 32 lines per instruction costs
       // the single-evaluation modes a factor 1.9.)  The grid is warp-uniform:
       // a warp's teams share one segment.
       if constexpr (MODE == MODE_MIN || QUAT) {

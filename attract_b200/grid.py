@@ -296,7 +296,7 @@ class Grid:
         The pairs found do not depend on ``nb_refine``; a finer list grid visits
         fewer entries beyond the plateau (2: ~19 % fewer than 1, 4: another
         ~10 % fewer than 2) for 8x / 64x the record memory of the inner grid
-        (config-1 receptor: 0.36 GB at 2, 2.9 GB at 4).
+        (a 2500-bead receptor in a 40 A sphere: 0.36 GB at 2, 2.9 GB at 4).
         """
         dev = _dev(device)
         lib = _lib.load()
